@@ -1,0 +1,133 @@
+// extern "C" entry points of libbwpm_b200.so (declared in include/bwpm_b200.h).
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+
+#include "../../include/bwpm_b200.h"
+#include "solver.hpp"
+
+struct bwpm_solver {
+  std::unique_ptr<bwpm::Solver> impl;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return BWPM_OK;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return BWPM_EINVAL;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return BWPM_ERUNTIME;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return BWPM_ERUNTIME;
+  }
+}
+
+const bwpm::cd* as_cd(const double* p) { return reinterpret_cast<const bwpm::cd*>(p); }
+bwpm::cd* as_cd(double* p) { return reinterpret_cast<bwpm::cd*>(p); }
+
+}  // namespace
+
+extern "C" {
+
+size_t bwpm_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    const size_t k = std::min(len - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), k);
+    buf[k] = '\0';
+  }
+  return g_last_error.size();
+}
+
+const char* bwpm_version(void) { return "bwpm_b200 0.1 sm_100a"; }
+
+int bwpm_cuda_device_count(void) { return bwpm::device_count(); }
+
+int bwpm_interface_matrices(int reflection, const double* k_x, const double* k_y, size_t n,
+                            double in_re, double in_im, double out_re, double out_im, double k0,
+                            double* out) {
+  return guarded([&] {
+    if (n && (!k_x || !k_y || !out)) throw bwpm::invalid_argument("null array");
+    bwpm::interface_matrices(reflection, k_x, k_y, n, bwpm::cd{in_re, in_im},
+                             bwpm::cd{out_re, out_im}, k0, as_cd(out));
+  });
+}
+
+int bwpm_longitudinal_wavenumber(double index_re, double index_im, double k0,
+                                 const double* k_perp_sq, size_t n, double* out) {
+  return guarded([&] {
+    if (n && (!k_perp_sq || !out)) throw bwpm::invalid_argument("null array");
+    bwpm::longitudinal_wavenumbers(bwpm::cd{index_re, index_im}, k0, k_perp_sq, n, as_cd(out));
+  });
+}
+
+int bwpm_solver_create(size_t ny, size_t nx, double dy, double dx, double dz, double k0,
+                       const double* indices, size_t m, const int32_t* labels, size_t nz,
+                       double ib_re, double ib_im, const double* mask, int device,
+                       const double* fluctuation, int precision, double gmres_tol,
+                       bwpm_solver** out) {
+  return guarded([&] {
+    if (!out) throw bwpm::invalid_argument("null output handle");
+    *out = nullptr;
+    bwpm::SolverInput in;
+    in.ny = ny;
+    in.nx = nx;
+    in.dy = dy;
+    in.dx = dx;
+    in.dz = dz;
+    in.k0 = k0;
+    in.indices.assign(as_cd(indices), as_cd(indices) + m);
+    in.labels.assign(labels, labels + nz * ny * nx);
+    in.nz = nz;
+    in.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) in.mask.assign(mask, mask + ny * nx);
+    if (fluctuation) in.fluct.assign(as_cd(fluctuation), as_cd(fluctuation) + nz * ny * nx);
+    in.device = device;
+    in.gmres_tol = gmres_tol;
+    auto s = std::make_unique<bwpm_solver>();
+    s->impl = bwpm::make_plane_solver(std::move(in), precision);
+    *out = s.release();
+  });
+}
+
+int bwpm_solver_run(bwpm_solver* s, const double* field, int iterations, const int64_t* keep,
+                    size_t nkeep, double* transmitted, double* reflected, double* t_iter,
+                    double* r_iter, double* forward, double* backward, int64_t* stored_values) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null solver");
+    if (!field) throw bwpm::invalid_argument("field must have shape (ny, nx, 2)");
+    if (iterations < 0) throw bwpm::invalid_argument("iterations must be >= 0");
+    bwpm::RunOutputs o;
+    o.transmitted = as_cd(transmitted);
+    o.reflected = as_cd(reflected);
+    o.transmitted_iter = as_cd(t_iter);
+    o.reflected_iter = as_cd(r_iter);
+    o.forward = as_cd(forward);
+    o.backward = as_cd(backward);
+    s->impl->run(as_cd(field), iterations, keep, nkeep, o);
+    if (stored_values) *stored_values = o.stored_values;
+  });
+}
+
+int bwpm_solver_stats(const bwpm_solver* s, int64_t* device_bytes, int64_t* kernel_launches,
+                      int64_t* gmres_applies) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null solver");
+    if (device_bytes) *device_bytes = static_cast<int64_t>(s->impl->device_bytes());
+    if (kernel_launches) *kernel_launches = s->impl->kernel_launches();
+    if (gmres_applies) *gmres_applies = s->impl->gmres_applies();
+  });
+}
+
+void bwpm_solver_destroy(bwpm_solver* s) { delete s; }
+
+}  // extern "C"

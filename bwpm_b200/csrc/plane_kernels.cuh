@@ -1,0 +1,285 @@
+// Slab-step kernels of the plane engine (general ny × nx planes, FP64 or FP32 complex).
+//
+// One slab step (cpp/src/solver.cpp:384-417, "apply") for a field e of shape (ny, nx, 2):
+//   out = mask · Σ_(r,s) I_r,s · F⁻¹{M_rs · F{e}}   (transmission kinds)
+//   vals[j] = [Σ_(r,s), ñ_r≠ñ_s I_r,s · F⁻¹{R_rs · F{e}}](iface[j])   (reflection kinds)
+// The forward transform is shared by the reflection and the transmission of the same step
+// (the reference computes it twice), every (pair, kind) is one "pass" of spectral multiply and
+// inverse transform, and the pixel selection I_r,s, the mask, the gather of reflection sources
+// at interface pixels and the sparse source add of cpp/src/solver.cpp:419-441 run in the
+// epilogue of the inverse transform.
+//
+// 2D (nx = 1): the matrices are diagonal (k_x = 0 exactly), so E_x and E_y are independent;
+// k_step2d runs one CTA per component and does the whole step in shared memory.
+// 3D: k_rows_fft (x transform), k_cols_step (y transform, passes, inverse y transform) and
+// k_rows_select (inverse x transform + epilogue).
+#pragma once
+
+#include "fft.cuh"
+#include "interface.cuh"
+
+namespace bwpm {
+
+constexpr int kMaxPasses = 128;
+
+// Pass j of a step: pair index (into the step's pair-id plane), operator table, reflection flag.
+struct StepPasses {
+  int npass = 0;
+  int pair[kMaxPasses];
+  const void* tab[kMaxPasses];  // (m00, m01, m11) SoA operator table, 3·N entries of cx<T>
+  int refl[kMaxPasses];
+};
+
+template <typename T>
+struct Step2D {
+  const cx<T>* in;          // (N, 2)
+  cx<T>* out;               // (N, 2)
+  cx<T>* spec;              // (N, 2) spectrum scratch F{e}
+  const uint8_t* pid;       // (N) pair id per pixel, or null when the step has one pair
+  const T* mask;            // (N) or null
+  const int* iface;         // sorted interface pixels of the step, or null
+  int niface;
+  cx<T>* refl_out;          // (niface, 2) gathered reflection sources, or null
+  const cx<T>* add;         // (niface, 2) sparse sources added after the step, or null
+  int n;
+  int store_spec;           // keep F{e} in `spec` even for a single pass (Born)
+  T inv_n;
+};
+
+template <typename T>
+__global__ void k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const cx<T>* __restrict__ tw) {
+  extern __shared__ unsigned char smem_raw[];
+  cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
+  const int c = blockIdx.x;
+  const int n = a.n, tid = threadIdx.x, nt = blockDim.x;
+  for (int q = tid; q < n; q += nt) buf[q] = a.in[2 * q + c];
+  __syncthreads();
+  fft_smem<-1>(buf, plan, tw, 1, tid, nt);
+  cx<T>* spec = a.spec;  // interleaved (N, 2), like the field
+  const bool keep_spec = ps.npass > 1 || a.store_spec;
+  if (keep_spec) {
+    for (int q = tid; q < n; q += nt) spec[2 * q + c] = buf[q];
+    __syncthreads();
+  }
+  const long long e = c == 0 ? 0 : 2LL * n;  // m00 for E_x, m11 for E_y
+  for (int j = 0; j < ps.npass; ++j) {
+    const cx<T>* m = static_cast<const cx<T>*>(ps.tab[j]) + e;
+    if (keep_spec)
+      for (int q = tid; q < n; q += nt) buf[q] = spec[2 * q + c] * m[q];
+    else
+      for (int q = tid; q < n; q += nt) buf[q] = buf[q] * m[q];
+    __syncthreads();
+    fft_smem<+1>(buf, plan, tw, 1, tid, nt);
+    const int pair = ps.pair[j];
+    if (!ps.refl[j]) {
+      for (int q = tid; q < n; q += nt)
+        if (!a.pid || a.pid[q] == pair) {
+          cx<T> v = buf[q] * a.inv_n;
+          if (a.mask) v = v * a.mask[q];
+          a.out[2 * q + c] = v;
+        }
+    } else {
+      for (int k = tid; k < a.niface; k += nt) {
+        const int q = a.iface[k];
+        if (!a.pid || a.pid[q] == pair) a.refl_out[2 * k + c] = buf[q] * a.inv_n;
+      }
+    }
+    __syncthreads();
+  }
+  if (a.add)
+    for (int k = tid; k < a.niface; k += nt) {
+      const int q = a.iface[k];
+      a.out[2 * q + c] = a.out[2 * q + c] + a.add[2 * k + c];
+    }
+}
+
+// x transform of `rows` rows × ncomp interleaved components per CTA; smem [x][row][comp].
+template <int DIR, typename T>
+__global__ void k_rows_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int rows,
+                           FftPlan plan, const cx<T>* __restrict__ tw) {
+  extern __shared__ unsigned char smem_raw[];
+  cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
+  const int y0 = blockIdx.x * rows;
+  const int here = min(rows, ny - y0);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int per_row = nx * ncomp;
+  const int total = rows * per_row;
+  for (int idx = tid; idx < total; idx += nt) {
+    const int row = idx / per_row, rem = idx - row * per_row;
+    const int x = rem / ncomp, c = rem - x * ncomp;
+    buf[(x * rows + row) * ncomp + c] =
+        row < here ? in[(static_cast<long long>(y0 + row) * nx + x) * ncomp + c] : cx<T>{0, 0};
+  }
+  __syncthreads();
+  fft_smem<DIR>(buf, plan, tw, rows * ncomp, tid, nt);
+  for (int idx = tid; idx < here * per_row; idx += nt) {
+    const int row = idx / per_row, rem = idx - row * per_row;
+    const int x = rem / ncomp, c = rem - x * ncomp;
+    out[(static_cast<long long>(y0 + row) * nx + x) * ncomp + c] = buf[(x * rows + row) * ncomp + c];
+  }
+}
+
+template <typename T>
+struct ColStep {
+  const cx<T>* in;      // x-transformed field (N, 2)
+  cx<T>* work;          // npass planes (N, 2)
+  cx<T>* spec_out;      // full spectrum F{e} (N, 2), or null
+  int ny, nx, cols;
+};
+
+// y transform of a tile of `cols` columns, then per pass: W = M·Ŝ (2×2), inverse y transform,
+// store to work plane j. smem: spectrum tile [y][col][2] and, for several passes, a work tile.
+template <typename T>
+__global__ void k_cols_step(ColStep<T> a, StepPasses ps, FftPlan plan,
+                            const cx<T>* __restrict__ tw) {
+  extern __shared__ unsigned char smem_raw[];
+  cx<T>* sbuf = reinterpret_cast<cx<T>*>(smem_raw);
+  const int ny = a.ny, nx = a.nx, cols = a.cols;
+  const long long n = static_cast<long long>(ny) * nx;
+  const int tile = ny * cols * 2;
+  cx<T>* wbuf = ps.npass > 1 ? sbuf + tile : sbuf;
+  const int x0 = blockIdx.x * cols;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int idx = tid; idx < tile; idx += nt) {
+    const int y = idx / (2 * cols), rem = idx - y * 2 * cols;
+    const int xc = rem >> 1, c = rem & 1;
+    const int x = x0 + xc;
+    sbuf[idx] = x < nx ? a.in[(static_cast<long long>(y) * nx + x) * 2 + c] : cx<T>{0, 0};
+  }
+  __syncthreads();
+  fft_smem<-1>(sbuf, plan, tw, 2 * cols, tid, nt);
+  if (a.spec_out)
+    for (int idx = tid; idx < tile; idx += nt) {
+      const int y = idx / (2 * cols), rem = idx - y * 2 * cols;
+      const int x = x0 + (rem >> 1);
+      if (x < nx) a.spec_out[(static_cast<long long>(y) * nx + x) * 2 + (rem & 1)] = sbuf[idx];
+    }
+  for (int j = 0; j < ps.npass; ++j) {
+    const cx<T>* m = static_cast<const cx<T>*>(ps.tab[j]);
+    for (int idx = tid; idx < ny * cols; idx += nt) {
+      const int y = idx / cols, xc = idx - y * cols;
+      const int x = x0 + xc;
+      if (x >= nx) {
+        wbuf[2 * idx] = cx<T>{0, 0};
+        wbuf[2 * idx + 1] = cx<T>{0, 0};
+        continue;
+      }
+      const long long q = static_cast<long long>(y) * nx + x;
+      const cx<T> m00 = m[q], m01 = m[n + q], m11 = m[2 * n + q];
+      const cx<T> s0 = sbuf[2 * idx], s1 = sbuf[2 * idx + 1];
+      wbuf[2 * idx] = m00 * s0 + m01 * s1;
+      wbuf[2 * idx + 1] = m01 * s0 + m11 * s1;
+    }
+    __syncthreads();
+    fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
+    cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
+    for (int idx = tid; idx < tile; idx += nt) {
+      const int y = idx / (2 * cols), rem = idx - y * 2 * cols;
+      const int x = x0 + (rem >> 1);
+      if (x < nx) w[(static_cast<long long>(y) * nx + x) * 2 + (rem & 1)] = wbuf[idx];
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+struct RowSelect {
+  const cx<T>* work;        // npass planes (N, 2) after the inverse y transform
+  cx<T>* out;               // (N, 2)
+  const uint8_t* pid;       // or null
+  const T* mask;            // or null
+  const int* iface;         // interface pixels of the step (sorted), or null
+  const int* rowoff;        // (ny + 1) offsets into iface per row
+  cx<T>* refl_out;          // (niface, 2) or null
+  const cx<T>* add;         // (niface, 2) or null
+  int ny, nx, rows;
+  T inv_n;
+};
+
+// inverse x transform of each pass for `rows` rows, then select/mask/gather/add.
+template <typename T>
+__global__ void k_rows_select(RowSelect<T> a, StepPasses ps, FftPlan plan,
+                              const cx<T>* __restrict__ tw) {
+  extern __shared__ unsigned char smem_raw[];
+  cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
+  const int ny = a.ny, nx = a.nx, rows = a.rows;
+  const long long n = static_cast<long long>(ny) * nx;
+  const int y0 = blockIdx.x * rows;
+  const int here = min(rows, ny - y0);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int per_row = nx * 2, total = rows * per_row;
+  const int k0 = a.iface ? a.rowoff[y0] : 0, k1 = a.iface ? a.rowoff[y0 + here] : 0;
+  for (int j = 0; j < ps.npass; ++j) {
+    const cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
+    for (int idx = tid; idx < total; idx += nt) {
+      const int row = idx / per_row, rem = idx - row * per_row;
+      const int x = rem >> 1, c = rem & 1;
+      buf[(x * rows + row) * 2 + c] =
+          row < here ? w[(static_cast<long long>(y0 + row) * nx + x) * 2 + c] : cx<T>{0, 0};
+    }
+    __syncthreads();
+    fft_smem<+1>(buf, plan, tw, 2 * rows, tid, nt);
+    const int pair = ps.pair[j];
+    if (!ps.refl[j]) {
+      for (int idx = tid; idx < here * per_row; idx += nt) {
+        const int row = idx / per_row, rem = idx - row * per_row;
+        const int x = rem >> 1, c = rem & 1;
+        const long long q = static_cast<long long>(y0 + row) * nx + x;
+        if (!a.pid || a.pid[q] == pair) {
+          cx<T> v = buf[(x * rows + row) * 2 + c] * a.inv_n;
+          if (a.mask) v = v * a.mask[q];
+          a.out[2 * q + c] = v;
+        }
+      }
+    } else {
+      for (int k = k0 + tid; k < k1; k += nt) {
+        const int q = a.iface[k];
+        if (a.pid && a.pid[q] != pair) continue;
+        const int row = q / nx - y0, x = q - (q / nx) * nx;
+        a.refl_out[2 * k] = buf[(x * rows + row) * 2] * a.inv_n;
+        a.refl_out[2 * k + 1] = buf[(x * rows + row) * 2 + 1] * a.inv_n;
+      }
+    }
+    __syncthreads();
+  }
+  if (a.add)
+    for (int k = k0 + tid; k < k1; k += nt) {
+      const int q = a.iface[k];
+      a.out[2 * q] = a.out[2 * q] + a.add[2 * k];
+      a.out[2 * q + 1] = a.out[2 * q + 1] + a.add[2 * k + 1];
+    }
+}
+
+// ---- small helpers ------------------------------------------------------------------------
+
+template <typename T>
+__global__ void k_add_plane(cx<T>* dst, const cx<T>* src, const T* mask, T scale, long long n2) {
+  // dst += src·scale (· mask per pixel when given); n2 = complex entries of an (N, 2) plane
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= n2) return;
+  const cx<T> s = mask ? src[i] * (scale * mask[i >> 1]) : src[i] * scale;
+  dst[i] = dst[i] + s;
+}
+
+template <typename To, typename From>
+__global__ void k_convert(cx<To>* dst, const cx<From>* src, long long count) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i < count) dst[i] = cast<To>(src[i]);
+}
+
+template <typename T>
+__global__ void k_build_table(cx<T>* out, int kind, cd nr, cd ns, int ny, int nx, double dy,
+                              double dx, double k0, double dz) {
+  const long long n = static_cast<long long>(ny) * nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q >= n) return;
+  const double kx = fftfreq(q % nx, nx, dx);
+  const double ky = fftfreq(q / nx, ny, dy);
+  cd m[3];
+  operator_matrix(kind, kx, ky, nr, ns, k0, dz, m);
+  out[q] = cast<T>(m[0]);
+  out[n + q] = cast<T>(m[1]);
+  out[2 * n + q] = cast<T>(m[2]);
+}
+
+}  // namespace bwpm

@@ -1,0 +1,809 @@
+// Plane engine: the drop-in CudaSolver (FP64) and its complex64 twin, general ny × nx planes.
+//
+// Same algorithm, inputs and outputs as the reference's bwpm::CudaSolver / bwpm::Solver
+// (cpp/src/solver_cuda.cu:643-853, cpp/src/solver.cpp:27-528), re-designed for the device:
+// - labels become per-step uint8 pair-id planes (deduplicated), resident on the device;
+// - operator tables T/R × propagator are built once per (kind, ñ_r, ñ_s) in FP64 on the device
+//   (the reference recomputes them in every kernel call) and stored in the field precision;
+// - one forward transform per step feeds both the reflection and the transmission;
+// - selection, mask, reflection gather and sparse source add are fused into the inverse
+//   transform's epilogue; interface pixel lists and source stores are allocated once.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+
+#include "born_kernels.cuh"
+#include "plan.hpp"
+#include "plane_kernels.cuh"
+#include "solver.hpp"
+
+namespace bwpm {
+namespace {
+
+template <typename U>
+struct DevBuf {
+  U* ptr = nullptr;
+  std::size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(std::size_t count) { alloc(count); }
+  void alloc(std::size_t count) {
+    release();
+    n = count;
+    if (count) check_cuda(cudaMalloc(&ptr, count * sizeof(U)), "cudaMalloc");
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { release(); }
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), n(o.n) {
+    o.ptr = nullptr;
+    o.n = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    std::swap(ptr, o.ptr);
+    std::swap(n, o.n);
+    return *this;
+  }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  std::size_t bytes() const { return n * sizeof(U); }
+};
+
+constexpr int kThreads = 256;
+
+struct StepInfo {
+  std::vector<std::pair<int, int>> pairs;  // (label at plane p, label at plane p + 1), sorted
+  long long pid_off = -1;                  // offset into the pair-id pool, −1: a single pair
+  long long iface_off = 0;
+  int niface = 0;
+  long long rowoff_off = -1;               // 3D: offsets of each row into the interface list
+  int host_slot = -1;                      // Born slab: index into the host/potential arrays
+};
+
+struct LaunchShape {
+  int rows = 1, threads = 32;
+  std::size_t smem = 0;
+};
+
+template <typename T>
+class PlaneSolver final : public Solver {
+ public:
+  explicit PlaneSolver(SolverInput in) : in_(std::move(in)) { setup(); }
+  ~PlaneSolver() override {
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  void run(const cd* field, int iterations, const std::int64_t* keep, std::size_t nkeep,
+           RunOutputs& out) override;
+  std::size_t device_bytes() const override;
+  std::int64_t kernel_launches() const override { return launches_; }
+  std::int64_t gmres_applies() const override { return gmres_applies_; }
+
+ private:
+  using C = cx<T>;
+  void setup();
+  const C* table(int kind, cd nr, cd ns);
+  StepPasses passes(int step, bool backward, bool reflect);
+  void step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out, const C* add,
+            bool want_spec);
+  void fft_plane(const C* in, C* out, int ncomp, int dir);
+  void born_operator(const C* in, C* out, int slot, int dir);
+  void born_step(const C* spec, C* inc, int slot, int dir);
+  void born_sources(const C* spec, int slot, int dir);
+  void born_emission(int slot, int dir, C* plane);
+  void gmres(int slot, int dir);
+  cd dot(const C* u, const C* v, long long m);
+  void axpby(C* y, const C* x, cd a, cd b, long long m);
+  void add_plane_scaled(C* dst, const C* src, const T* mask);
+  LaunchShape rows_shape(int ncomp, int rows_max) const;
+  LaunchShape cols_shape(int ncomp, int tiles) const;
+  std::size_t n() const { return in_.ny * in_.nx; }
+  bool is2d() const { return in_.nx == 1; }
+  cd index_of(int label) const {
+    return label < 0 ? in_.index_before : in_.indices[static_cast<std::size_t>(label)];
+  }
+  BornGrid born_grid(int slot) const {
+    return BornGrid{hosts_[slot], in_.k0, in_.dz, in_.dy, in_.dx, static_cast<int>(in_.ny),
+                    static_cast<int>(in_.nx)};
+  }
+  template <typename K, typename... A>
+  void launch(K kernel, dim3 grid, dim3 block, std::size_t smem, A... args) {
+    kernel<<<grid, block, smem, stream_>>>(args...);
+    check_cuda(cudaGetLastError(), "kernel launch");
+    ++launches_;
+  }
+
+  SolverInput in_;
+  cudaStream_t stream_ = nullptr;
+  HostPlan hy_, hx_;
+  DevBuf<C> tw_y_, tw_x_;
+  std::vector<StepInfo> steps_;
+  DevBuf<std::uint8_t> pid_pool_;
+  DevBuf<int> iface_pool_, rowoff_pool_;
+  long long iface_total_ = 0;
+  DevBuf<T> mask_;
+  std::map<std::tuple<int, double, double, double, double>, DevBuf<C>> tables_;
+  // fields
+  DevBuf<C> input_, e_, next_, spec_, xbuf_, work_, src_fwd_, src_bwd_;
+  DevBuf<cd> stage_;
+  int max_pass_ = 1;
+  // Born
+  std::vector<cd> hosts_;
+  DevBuf<C> pot_, born_fwd_, born_bwd_, w3_, t3_, sources_, g_x_, g_rhs_, g_y_, g_w_, g_tmp_,
+      inc_;
+  std::vector<DevBuf<C>> basis_;
+  DevBuf<cd> partial_;
+  std::vector<cd> partial_host_;
+  // launch shapes
+  int thr2d_ = 32, thr_line3_ = 32;
+  LaunchShape rows2_, rows3_, sel_, cols1_, cols2_, cols3_;
+  std::int64_t launches_ = 0, gmres_applies_ = 0;
+};
+
+template <typename T>
+LaunchShape PlaneSolver<T>::rows_shape(int ncomp, int rows_max) const {
+  LaunchShape s;
+  const std::size_t row_bytes = in_.nx * ncomp * sizeof(C);
+  s.rows = static_cast<int>(std::max<std::size_t>(1, std::min<std::size_t>(rows_max, 49152 / row_bytes)));
+  while (s.rows > 1 && threads_needed(hx_.plan, s.rows * ncomp) > 1024) --s.rows;
+  s.threads = std::max(64, threads_needed(hx_.plan, s.rows * ncomp));
+  if (s.threads > 1024) throw invalid_argument("nx too large for the row transform");
+  s.smem = s.rows * row_bytes;
+  return s;
+}
+
+template <typename T>
+LaunchShape PlaneSolver<T>::cols_shape(int ncomp, int tiles) const {
+  LaunchShape s;
+  const std::size_t col_bytes = in_.ny * ncomp * sizeof(C);
+  int cols = std::max(1, static_cast<int>(64 / (ncomp * sizeof(C))));
+  while (cols > 1 && (col_bytes * cols * tiles > 98304 ||
+                      threads_needed(hy_.plan, cols * ncomp) > 1024))
+    --cols;
+  s.rows = cols;
+  s.threads = std::max(64, threads_needed(hy_.plan, cols * ncomp));
+  s.smem = col_bytes * cols * tiles;
+  if (s.threads > 1024 || s.smem > 227 * 1024)
+    throw invalid_argument("ny too large for the column transform");
+  return s;
+}
+
+template <typename T>
+void PlaneSolver<T>::setup() {
+  const std::size_t nn = n();
+  if (in_.ny < 1 || in_.nx < 1) throw invalid_argument("ny and nx must be positive");
+  if (in_.labels.size() != in_.nz * nn) throw invalid_argument("labels must have shape (nz, ny, nx)");
+  if (!in_.mask.empty() && in_.mask.size() != nn) throw invalid_argument("mask must have shape (ny, nx)");
+  for (auto l : in_.labels)
+    if (l < 0 || static_cast<std::size_t>(l) >= in_.indices.size())
+      throw invalid_argument("labels must index into `indices`");
+  if (nn > (1u << 30)) throw invalid_argument("plane too large");
+  // Born hosts per slab (cpp/src/solver.cpp:49-62)
+  std::vector<int> host_of(in_.nz, -1);
+  if (!in_.fluct.empty()) {
+    if (in_.fluct.size() != in_.nz * nn)
+      throw invalid_argument("fluctuation must have the shape of labels (nz, ny, nx)");
+    for (std::size_t j = 0; j < in_.nz; ++j) {
+      bool has = false;
+      cd host{0.0, 0.0};
+      for (std::size_t q = 0; q < nn; ++q) {
+        const cd d = in_.fluct[j * nn + q];
+        if (d.re == 0.0 && d.im == 0.0) continue;
+        const cd idx = in_.indices[static_cast<std::size_t>(in_.labels[j * nn + q])];
+        if (has && (host.re != idx.re || host.im != idx.im))
+          throw invalid_argument("slab " + std::to_string(j) + ": fluctuation must lie in one host index");
+        has = true;
+        host = idx;
+      }
+      if (has) {
+        host_of[j] = static_cast<int>(hosts_.size());
+        hosts_.push_back(host);
+      }
+    }
+  }
+  check_cuda(cudaSetDevice(in_.device), "cudaSetDevice");
+  check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  hy_ = make_plan(static_cast<int>(in_.ny));
+  hx_ = make_plan(static_cast<int>(in_.nx));
+  auto upload_tw = [&](const HostPlan& hp, DevBuf<C>& d) {
+    std::vector<C> t(hp.twiddles.size());
+    for (std::size_t i = 0; i < t.size(); ++i) t[i] = cast<T>(hp.twiddles[i]);
+    d.alloc(t.size());
+    check_cuda(cudaMemcpy(d.ptr, t.data(), t.size() * sizeof(C), cudaMemcpyHostToDevice), "twiddles");
+  };
+  upload_tw(hy_, tw_y_);
+  upload_tw(hx_, tw_x_);
+
+  // per-step pairs, pair-id planes (deduplicated), interface lists
+  std::vector<std::uint8_t> pid_host;
+  std::unordered_map<std::uint64_t, std::vector<long long>> pid_seen;
+  std::vector<int> iface_host, rowoff_host;
+  std::vector<std::int32_t> before(nn, -1);
+  steps_.resize(in_.nz);
+  std::vector<std::uint8_t> pid(nn);
+  for (std::size_t p = 0; p < in_.nz; ++p) {
+    const std::int32_t* a = p == 0 ? before.data() : in_.labels.data() + (p - 1) * nn;
+    const std::int32_t* b = in_.labels.data() + p * nn;
+    std::set<std::pair<int, int>> ps;
+    for (std::size_t q = 0; q < nn; ++q) ps.emplace(a[q], b[q]);
+    StepInfo& st = steps_[p];
+    st.pairs.assign(ps.begin(), ps.end());
+    if (st.pairs.size() > 255) throw invalid_argument("more than 255 label pairs in one step");
+    if (2 * st.pairs.size() > static_cast<std::size_t>(kMaxPasses))
+      throw invalid_argument("too many label pairs in one step");
+    if (st.pairs.size() > 1) {
+      std::map<std::pair<int, int>, int> id;
+      for (std::size_t i = 0; i < st.pairs.size(); ++i) id[st.pairs[i]] = static_cast<int>(i);
+      std::uint64_t h = 1469598103934665603ULL;
+      for (std::size_t q = 0; q < nn; ++q) {
+        pid[q] = static_cast<std::uint8_t>(id[{a[q], b[q]}]);
+        h = (h ^ pid[q]) * 1099511628211ULL;
+      }
+      long long found = -1;
+      for (long long off : pid_seen[h])
+        if (std::memcmp(pid_host.data() + off, pid.data(), nn) == 0) {
+          found = off;
+          break;
+        }
+      if (found < 0) {
+        found = static_cast<long long>(pid_host.size());
+        pid_host.insert(pid_host.end(), pid.begin(), pid.end());
+        pid_seen[h].push_back(found);
+      }
+      st.pid_off = found;
+    }
+    st.iface_off = static_cast<long long>(iface_host.size());
+    for (std::size_t q = 0; q < nn; ++q) {
+      const cd x = index_of(a[q]), y = index_of(b[q]);
+      if (x.re != y.re || x.im != y.im) iface_host.push_back(static_cast<int>(q));
+    }
+    st.niface = static_cast<int>(iface_host.size() - st.iface_off);
+    if (st.niface > 0 && !is2d()) {
+      st.rowoff_off = static_cast<long long>(rowoff_host.size());
+      const int* first = iface_host.data() + st.iface_off;
+      for (std::size_t y = 0; y <= in_.ny; ++y)
+        rowoff_host.push_back(static_cast<int>(
+            std::lower_bound(first, first + st.niface, static_cast<int>(y * in_.nx)) - first));
+    }
+    st.host_slot = host_of[p];
+    int npass = static_cast<int>(st.pairs.size());
+    for (auto& pr : st.pairs) {
+      const cd x = index_of(pr.first), y = index_of(pr.second);
+      if (x.re != y.re || x.im != y.im) ++npass;
+    }
+    max_pass_ = std::max(max_pass_, npass);
+  }
+  iface_total_ = static_cast<long long>(iface_host.size());
+  if (!pid_host.empty()) {
+    pid_pool_.alloc(pid_host.size());
+    check_cuda(cudaMemcpy(pid_pool_.ptr, pid_host.data(), pid_host.size(), cudaMemcpyHostToDevice), "pid");
+  }
+  if (!iface_host.empty()) {
+    iface_pool_.alloc(iface_host.size());
+    check_cuda(cudaMemcpy(iface_pool_.ptr, iface_host.data(), iface_host.size() * sizeof(int),
+                          cudaMemcpyHostToDevice), "iface");
+    src_fwd_.alloc(2 * iface_host.size());
+    src_bwd_.alloc(2 * iface_host.size());
+  }
+  if (!rowoff_host.empty()) {
+    rowoff_pool_.alloc(rowoff_host.size());
+    check_cuda(cudaMemcpy(rowoff_pool_.ptr, rowoff_host.data(), rowoff_host.size() * sizeof(int),
+                          cudaMemcpyHostToDevice), "rowoff");
+  }
+  if (!in_.mask.empty()) {
+    std::vector<T> m(in_.mask.begin(), in_.mask.end());
+    mask_.alloc(nn);
+    check_cuda(cudaMemcpy(mask_.ptr, m.data(), nn * sizeof(T), cudaMemcpyHostToDevice), "mask");
+  }
+  input_.alloc(2 * nn);
+  e_.alloc(2 * nn);
+  next_.alloc(2 * nn);
+  spec_.alloc(2 * nn);
+  stage_.alloc(2 * nn);
+  // launch shapes and shared-memory opt-in
+  if (is2d()) {
+    thr2d_ = std::max(64, threads_needed(hy_.plan, 1));
+    if (thr2d_ > 1024 || nn * sizeof(C) > 227 * 1024)
+      throw invalid_argument("ny too large for the single-CTA line transform");
+    thr_line3_ = thr2d_;
+    check_cuda(cudaFuncSetAttribute(k_step2d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+    check_cuda(cudaFuncSetAttribute(k_line_fft<-1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+    check_cuda(cudaFuncSetAttribute(k_line_fft<1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+  } else {
+    rows2_ = rows_shape(2, 8);
+    rows3_ = rows_shape(3, 8);
+    sel_ = rows_shape(2, 8);
+    cols1_ = cols_shape(2, 1);
+    cols2_ = cols_shape(2, 2);
+    cols3_ = cols_shape(3, 1);
+    xbuf_.alloc(2 * nn);
+    work_.alloc(static_cast<std::size_t>(max_pass_) * 2 * nn);
+    for (auto k : {(const void*)k_rows_fft<-1, T>, (const void*)k_rows_fft<1, T>,
+                   (const void*)k_cols_step<T>, (const void*)k_rows_select<T>,
+                   (const void*)k_cols_fft<-1, T>, (const void*)k_cols_fft<1, T>})
+      check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+  }
+  // operator tables of the forward transmission (all runs need them)
+  for (std::size_t p = 0; p < in_.nz; ++p)
+    for (auto& pr : steps_[p].pairs) table(kFwdT, index_of(pr.first), index_of(pr.second));
+  // Born: potential V = 2ñ₀k₀²δn per host slab, full-plane source stores
+  if (!hosts_.empty()) {
+    pot_.alloc(hosts_.size() * nn);
+    DevBuf<cd> dn(nn);
+    std::vector<cd> v(nn);
+    for (std::size_t p = 0; p < in_.nz; ++p) {
+      const int slot = host_of[p];
+      if (slot < 0) continue;
+      const cd scale = ((2.0 * hosts_[slot]) * in_.k0) * in_.k0;  // cpp/src/solver.cpp:241
+      for (std::size_t q = 0; q < nn; ++q) v[q] = scale * in_.fluct[p * nn + q];
+      std::vector<C> vt(nn);
+      for (std::size_t q = 0; q < nn; ++q) vt[q] = cast<T>(v[q]);
+      check_cuda(cudaMemcpy(pot_.ptr + slot * nn, vt.data(), nn * sizeof(C), cudaMemcpyHostToDevice), "potential");
+    }
+    born_fwd_.alloc(hosts_.size() * 2 * nn);
+    born_bwd_.alloc(hosts_.size() * 2 * nn);
+    w3_.alloc(3 * nn);
+    t3_.alloc(3 * nn);
+    sources_.alloc(6 * nn);
+    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &inc_}) b->alloc(2 * nn);
+    partial_.alloc(1024);
+    partial_host_.resize(1024);
+  }
+  check_cuda(cudaDeviceSynchronize(), "setup");
+}
+
+template <typename T>
+const cx<T>* PlaneSolver<T>::table(int kind, cd nr, cd ns) {
+  auto key = std::make_tuple(kind, nr.re, nr.im, ns.re, ns.im);
+  auto it = tables_.find(key);
+  if (it != tables_.end()) return it->second.ptr;
+  DevBuf<C> t(3 * n());
+  launch(k_build_table<T>, dim3(ceil_div(n(), kThreads)), dim3(kThreads), 0, t.ptr, kind, nr, ns,
+         static_cast<int>(in_.ny), static_cast<int>(in_.nx), in_.dy, in_.dx, in_.k0, in_.dz);
+  const C* ptr = t.ptr;
+  tables_.emplace(key, std::move(t));
+  return ptr;
+}
+
+template <typename T>
+StepPasses PlaneSolver<T>::passes(int s, bool backward, bool reflect) {
+  // forward step s: (r, s) = (plane s, plane s + 1); backward step from plane s + 1 to plane s
+  // swaps the roles (cpp/src/solver_cuda.cu:615-624)
+  const StepInfo& st = steps_[s];
+  StepPasses ps;
+  ps.npass = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1 && !reflect) break;
+    for (std::size_t i = 0; i < st.pairs.size(); ++i) {
+      const int lr = backward ? st.pairs[i].second : st.pairs[i].first;
+      const int ls = backward ? st.pairs[i].first : st.pairs[i].second;
+      const cd nr = index_of(lr), ns = index_of(ls);
+      const bool same = nr.re == ns.re && nr.im == ns.im;
+      if (pass == 1 && same) continue;
+      const int kind = pass == 0 ? (backward ? kBwdT : kFwdT) : (backward ? kBwdR : kFwdR);
+      ps.pair[ps.npass] = static_cast<int>(i);
+      ps.tab[ps.npass] = table(kind, nr, ns);
+      ps.refl[ps.npass] = pass;
+      ++ps.npass;
+    }
+  }
+  return ps;
+}
+
+template <typename T>
+void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out,
+                          const C* add, bool want_spec) {
+  const StepInfo& st = steps_[s];
+  const StepPasses ps = passes(s, backward, reflect);
+  const std::uint8_t* pid = st.pid_off >= 0 ? pid_pool_.ptr + st.pid_off : nullptr;
+  const int* iface = st.niface > 0 ? iface_pool_.ptr + st.iface_off : nullptr;
+  const T inv_n = static_cast<T>(1.0 / static_cast<double>(n()));
+  if (is2d()) {
+    Step2D<T> a;
+    a.in = in;
+    a.out = out;
+    a.spec = spec_.ptr;
+    a.pid = pid;
+    a.mask = mask_.ptr;
+    a.iface = iface;
+    a.niface = st.niface;
+    a.refl_out = refl_out;
+    a.add = add;
+    a.n = static_cast<int>(n());
+    a.store_spec = want_spec ? 1 : 0;
+    a.inv_n = inv_n;
+    launch(k_step2d<T>, dim3(2), dim3(thr2d_), n() * sizeof(C), a, ps, hy_.plan, tw_y_.ptr);
+    return;
+  }
+  const int ny = static_cast<int>(in_.ny), nx = static_cast<int>(in_.nx);
+  launch(k_rows_fft<-1, T>, dim3(ceil_div(ny, rows2_.rows)), dim3(rows2_.threads), rows2_.smem, in,
+         xbuf_.ptr, ny, nx, 2, rows2_.rows, hx_.plan, tw_x_.ptr);
+  const LaunchShape& cs = ps.npass > 1 ? cols2_ : cols1_;
+  ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cs.rows};
+  launch(k_cols_step<T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem, c, ps, hy_.plan,
+         tw_y_.ptr);
+  RowSelect<T> r;
+  r.work = work_.ptr;
+  r.out = out;
+  r.pid = pid;
+  r.mask = mask_.ptr;
+  r.iface = iface;
+  r.rowoff = st.rowoff_off >= 0 ? rowoff_pool_.ptr + st.rowoff_off : nullptr;
+  r.refl_out = refl_out;
+  r.add = add;
+  r.ny = ny;
+  r.nx = nx;
+  r.rows = sel_.rows;
+  r.inv_n = inv_n;
+  launch(k_rows_select<T>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, r, ps,
+         hx_.plan, tw_x_.ptr);
+}
+
+template <typename T>
+void PlaneSolver<T>::fft_plane(const C* in, C* out, int ncomp, int dir) {
+  const int ny = static_cast<int>(in_.ny), nx = static_cast<int>(in_.nx);
+  if (is2d()) {
+    if (dir < 0)
+      launch(k_line_fft<-1, T>, dim3(ncomp), dim3(thr_line3_), n() * sizeof(C), in, out, ny, ncomp,
+             hy_.plan, tw_y_.ptr);
+    else
+      launch(k_line_fft<1, T>, dim3(ncomp), dim3(thr_line3_), n() * sizeof(C), in, out, ny, ncomp,
+             hy_.plan, tw_y_.ptr);
+    return;
+  }
+  const LaunchShape& rs = ncomp == 3 ? rows3_ : rows2_;
+  const LaunchShape& cs = ncomp == 3 ? cols3_ : cols1_;
+  C* tmp = ncomp == 3 ? t3_.ptr : xbuf_.ptr;
+  if (dir < 0) {
+    launch(k_rows_fft<-1, T>, dim3(ceil_div(ny, rs.rows)), dim3(rs.threads), rs.smem, in, tmp, ny,
+           nx, ncomp, rs.rows, hx_.plan, tw_x_.ptr);
+    launch(k_cols_fft<-1, T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem,
+           (const C*)tmp, out, ny, nx, ncomp, cs.rows, hy_.plan, tw_y_.ptr);
+  } else {
+    launch(k_rows_fft<1, T>, dim3(ceil_div(ny, rs.rows)), dim3(rs.threads), rs.smem, in, tmp, ny,
+           nx, ncomp, rs.rows, hx_.plan, tw_x_.ptr);
+    launch(k_cols_fft<1, T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem,
+           (const C*)tmp, out, ny, nx, ncomp, cs.rows, hy_.plan, tw_y_.ptr);
+  }
+}
+
+template <typename T>
+void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir) {
+  // cpp/src/solver.cpp:262-311
+  const BornGrid g = born_grid(slot);
+  const long long nn = static_cast<long long>(n());
+  launch(k_born_prepare<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, in, w3_.ptr, g, dir, 0.0);
+  fft_plane(w3_.ptr, w3_.ptr, 3, +1);
+  launch(k_born_potential<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr,
+         (const C*)(pot_.ptr + slot * nn), nn, static_cast<T>(1.0 / static_cast<double>(nn)));
+  fft_plane(w3_.ptr, w3_.ptr, 3, -1);
+  launch(k_born_finish<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, (const C*)w3_.ptr, out,
+         g, dir);
+}
+
+template <typename T>
+cd PlaneSolver<T>::dot(const C* u, const C* v, long long m) {
+  const int blocks = static_cast<int>(std::min<long long>(1024, (m + 255) / 256));
+  launch(k_dot_partial<T>, dim3(blocks), dim3(256), 0, u, v, m, partial_.ptr);
+  check_cuda(cudaMemcpyAsync(partial_host_.data(), partial_.ptr, blocks * sizeof(cd),
+                             cudaMemcpyDeviceToHost, stream_), "dot");
+  check_cuda(cudaStreamSynchronize(stream_), "dot");
+  cd s{0.0, 0.0};
+  for (int i = 0; i < blocks; ++i) s = s + partial_host_[i];
+  return s;
+}
+
+template <typename T>
+void PlaneSolver<T>::axpby(C* y, const C* x, cd a, cd b, long long m) {
+  launch(k_axpby<T>, dim3(ceil_div(m, kThreads)), dim3(kThreads), 0, y, x, a, b, m);
+}
+
+// dst += src/N (· mask): Born increments and emitted planes are kept unnormalised.
+template <typename T>
+void PlaneSolver<T>::add_plane_scaled(C* dst, const C* src, const T* mask) {
+  const long long n2 = 2 * static_cast<long long>(n());
+  launch(k_add_plane<T>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, dst, src, mask,
+         static_cast<T>(1.0 / static_cast<double>(n())), n2);
+}
+
+// GMRES(30) for (1 − G/2)·y = rhs with start y = rhs (cpp/src/solver.cpp:130-207, :336-342).
+template <typename T>
+void PlaneSolver<T>::gmres(int slot, int dir) {
+  const long long m2 = 2 * static_cast<long long>(n());
+  const int restart = 30;
+  const double tol = in_.gmres_tol;
+  if (basis_.empty())
+    for (int i = 0; i <= restart; ++i) basis_.emplace_back(static_cast<std::size_t>(m2));
+  auto apply = [&](const C* v, C* av) {  // av = v − G v/2
+    born_operator(v, g_tmp_.ptr, slot, dir);
+    ++gmres_applies_;
+    check_cuda(cudaMemcpyAsync(av, v, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+    axpby(av, g_tmp_.ptr, cd{-0.5, 0.0}, cd{1.0, 0.0}, m2);
+  };
+  auto norm = [&](const C* u) { return std::sqrt(dot(u, u, m2).re); };
+  check_cuda(cudaMemcpyAsync(g_y_.ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+  const double bnorm = norm(g_rhs_.ptr);
+  if (bnorm == 0.0) return;
+  const int m = restart;
+  std::vector<cd> h((m + 1) * m), gv(m + 1), cs(m), sn(m);
+  for (int outer = 0; outer < 100; ++outer) {
+    apply(g_y_.ptr, g_w_.ptr);
+    check_cuda(cudaMemcpyAsync(basis_[0].ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+    axpby(basis_[0].ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
+    const double beta = norm(basis_[0].ptr);
+    if (beta <= tol * bnorm) return;
+    axpby(basis_[0].ptr, basis_[0].ptr, cd{0.0, 0.0}, cd{1.0 / beta, 0.0}, m2);
+    std::fill(gv.begin(), gv.end(), cd{0.0, 0.0});
+    gv[0] = cd{beta, 0.0};
+    int used = 0;
+    bool done = false;
+    for (int j = 0; j < m; ++j) {
+      apply(basis_[j].ptr, g_w_.ptr);
+      for (int i = 0; i <= j; ++i) {
+        const cd hij = dot(basis_[i].ptr, g_w_.ptr, m2);
+        h[i * m + j] = hij;
+        axpby(g_w_.ptr, basis_[i].ptr, -hij, cd{1.0, 0.0}, m2);
+      }
+      const double hnext = norm(g_w_.ptr);
+      if (hnext > 0.0) {
+        check_cuda(cudaMemcpyAsync(basis_[j + 1].ptr, g_w_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+        axpby(basis_[j + 1].ptr, basis_[j + 1].ptr, cd{0.0, 0.0}, cd{1.0 / hnext, 0.0}, m2);
+      }
+      for (int i = 0; i < j; ++i) {
+        const cd a = h[i * m + j], c = h[(i + 1) * m + j];
+        h[i * m + j] = cs[i] * a + sn[i] * c;
+        h[(i + 1) * m + j] = -(conj(sn[i]) * a) + cs[i] * c;
+      }
+      const cd a = h[j * m + j];
+      const double aa = std::hypot(a.re, a.im);
+      const double r = std::sqrt(aa * aa + hnext * hnext);
+      if (aa == 0.0) {
+        cs[j] = cd{0.0, 0.0};
+        sn[j] = cd{1.0, 0.0};
+      } else {
+        cs[j] = cd{aa / r, 0.0};
+        sn[j] = (a / aa) * (hnext / r);
+      }
+      h[j * m + j] = cs[j] * a + sn[j] * hnext;
+      gv[j + 1] = -(conj(sn[j]) * gv[j]);
+      gv[j] = cs[j] * gv[j];
+      used = j + 1;
+      if (std::hypot(gv[j + 1].re, gv[j + 1].im) <= tol * bnorm || hnext == 0.0) {
+        done = true;
+        break;
+      }
+    }
+    std::vector<cd> y(used);
+    for (int i = used - 1; i >= 0; --i) {
+      cd s = gv[i];
+      for (int k = i + 1; k < used; ++k) s = s - h[i * m + k] * y[k];
+      y[i] = cdiv(s, h[i * m + i]);
+    }
+    for (int i = 0; i < used; ++i) axpby(g_y_.ptr, basis_[i].ptr, y[i], cd{1.0, 0.0}, m2);
+    if (done) {
+      apply(g_y_.ptr, g_w_.ptr);
+      check_cuda(cudaMemcpyAsync(g_tmp_.ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+      axpby(g_tmp_.ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
+      if (norm(g_tmp_.ptr) <= tol * bnorm * 10.0) return;
+    }
+  }
+  throw std::runtime_error("GMRES did not converge in the Born step (CUDA)");
+}
+
+// inc = F⁻¹{P_½^{±}·y}·N, (1 − G/2)y = G·P_½·F{e} (cpp/src/solver.cpp:313-350); the caller adds
+// inc/N (scaled in the add).
+template <typename T>
+void PlaneSolver<T>::born_step(const C* spec, C* inc, int slot, int dir) {
+  const BornGrid g = born_grid(slot);
+  const long long nn = static_cast<long long>(n());
+  launch(k_born_half<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, spec, g_x_.ptr, g, 1.0);
+  born_operator(g_x_.ptr, g_rhs_.ptr, slot, dir);
+  gmres(slot, dir);
+  launch(k_born_half<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, (const C*)g_y_.ptr,
+         g_y_.ptr, g, dir > 0 ? 1.0 : -1.0);
+  fft_plane(g_y_.ptr, inc, 2, +1);
+}
+
+// Ŝ_m = F{V·F⁻¹{e^{i k_z s_m}(Ê⊥, Ê_z)}} into sources_ (cpp/src/solver.cpp:215-260).
+template <typename T>
+void PlaneSolver<T>::born_sources(const C* spec, int slot, int dir) {
+  const BornGrid g = born_grid(slot);
+  const long long nn = static_cast<long long>(n());
+  const double r3 = 0.57735026918962576451;
+  const double gauss[2] = {(1.0 - r3) / 2.0, (1.0 + r3) / 2.0};
+  for (int m = 0; m < 2; ++m) {
+    const double dist = (dir > 0 ? gauss[m] : 1.0 - gauss[m]) * in_.dz;
+    launch(k_born_prepare<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, spec, w3_.ptr, g, dir, dist);
+    fft_plane(w3_.ptr, w3_.ptr, 3, +1);
+    launch(k_born_potential<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr,
+           (const C*)(pot_.ptr + slot * nn), nn, static_cast<T>(1.0 / static_cast<double>(nn)));
+    fft_plane(w3_.ptr, sources_.ptr + 3 * nn * m, 3, -1);
+  }
+}
+
+// Field radiated by sources_ in direction `dir` at the right slab edge, real space, times N
+// (cpp/src/solver.cpp:352-382); the caller scales by 1/N when adding.
+template <typename T>
+void PlaneSolver<T>::born_emission(int slot, int dir, C* plane) {
+  const BornGrid g = born_grid(slot);
+  const long long nn = static_cast<long long>(n());
+  launch(k_born_emit<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, (const C*)sources_.ptr,
+         inc_.ptr, g, dir);
+  fft_plane(inc_.ptr, plane, 2, +1);
+}
+
+template <typename T>
+void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* keep,
+                         std::size_t nkeep, RunOutputs& out) {
+  check_cuda(cudaSetDevice(in_.device), "cudaSetDevice");
+  const std::size_t nn = n();
+  const long long n2 = 2 * static_cast<long long>(nn);
+  const int nz = static_cast<int>(in_.nz);
+  const int iters = std::max(iterations, 1);
+  // keep planes: device slots
+  std::vector<int> keep_slot(nz + 1, -1);
+  for (std::size_t i = 0; i < nkeep; ++i)
+    if (keep[i] >= 0 && keep[i] <= nz) keep_slot[keep[i]] = static_cast<int>(i);
+  DevBuf<C> kept_f(nkeep * 2 * nn), kept_b(nkeep * 2 * nn), t_iter, r_iter;
+  if (iterations > 0) {
+    t_iter.alloc(iterations * 2 * nn);
+    r_iter.alloc(iterations * 2 * nn);
+  }
+  check_cuda(cudaMemcpyAsync(stage_.ptr, field, n2 * sizeof(cd), cudaMemcpyHostToDevice, stream_), "field upload");
+  launch(k_convert<T, double>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, input_.ptr,
+         (const cd*)stage_.ptr, n2);
+  auto copy = [&](C* dst, const C* src) {
+    check_cuda(cudaMemcpyAsync(dst, src, n2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+  };
+  C* e = e_.ptr;
+  C* next = next_.ptr;
+  const bool born = !hosts_.empty();
+  for (int it = 0; it < iters; ++it) {
+    const bool last = it == iters - 1;
+    copy(e, input_.ptr);
+    if (last && keep_slot[0] >= 0) copy(kept_f.ptr + keep_slot[0] * n2, e);
+    for (int p = 0; p < nz; ++p) {
+      const StepInfo& st = steps_[p];
+      const bool reflect = iterations > 0 && st.niface > 0;
+      const C* add = (it > 0 && st.niface > 0) ? src_fwd_.ptr + 2 * st.iface_off : nullptr;
+      const bool host = born && st.host_slot >= 0;
+      step(p, false, reflect, e, next, reflect ? src_bwd_.ptr + 2 * st.iface_off : nullptr, add, host);
+      if (host) {
+        born_step(spec_.ptr, inc_.ptr, st.host_slot, +1);
+        add_plane_scaled(next, inc_.ptr, mask_.ptr);
+        if (iterations > 0) {
+          born_sources(spec_.ptr, st.host_slot, +1);
+          born_emission(st.host_slot, -1, born_bwd_.ptr + st.host_slot * n2);  // born_bwd[p + 1]
+        }
+      }
+      std::swap(e, next);
+      if (it > 0 && host) add_plane_scaled(e, born_fwd_.ptr + st.host_slot * n2, nullptr);  // born_fwd[p + 1]
+      if (last && keep_slot[p + 1] >= 0) copy(kept_f.ptr + keep_slot[p + 1] * n2, e);
+    }
+    if (iterations > 0) copy(t_iter.ptr + it * n2, e);
+    if (iterations == 0) break;
+    check_cuda(cudaMemsetAsync(e, 0, n2 * sizeof(C), stream_), "memset");
+    if (born && steps_[nz - 1].host_slot >= 0)
+      add_plane_scaled(e, born_bwd_.ptr + steps_[nz - 1].host_slot * n2, nullptr);  // born_bwd[nz]
+    if (last && keep_slot[nz] >= 0) copy(kept_b.ptr + keep_slot[nz] * n2, e);
+    for (int p = nz; p > 0; --p) {
+      const StepInfo& st = steps_[p - 1];
+      if (born && st.host_slot >= 0) {
+        fft_plane(e, spec_.ptr, 2, -1);
+        born_sources(spec_.ptr, st.host_slot, -1);
+        born_emission(st.host_slot, +1, born_fwd_.ptr + st.host_slot * n2);  // born_fwd[p]
+        born_step(spec_.ptr, inc_.ptr, st.host_slot, -1);
+        add_plane_scaled(e, inc_.ptr, nullptr);  // R2 at plane p
+      }
+      const bool reflect = st.niface > 0;
+      const C* add = st.niface > 0 ? src_bwd_.ptr + 2 * st.iface_off : nullptr;
+      step(p - 1, true, reflect, e, next, reflect ? src_fwd_.ptr + 2 * st.iface_off : nullptr, add, false);
+      std::swap(e, next);
+      if (born && p >= 2 && steps_[p - 2].host_slot >= 0)
+        add_plane_scaled(e, born_bwd_.ptr + steps_[p - 2].host_slot * n2, nullptr);  // born_bwd[p − 1]
+      if (last && keep_slot[p - 1] >= 0) copy(kept_b.ptr + keep_slot[p - 1] * n2, e);
+    }
+    copy(r_iter.ptr + it * n2, e);
+  }
+  // outputs
+  auto download = [&](const C* src, cd* dst) {
+    if (!dst) return;
+    launch(k_convert<double, T>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, stage_.ptr, src, n2);
+    check_cuda(cudaMemcpyAsync(dst, stage_.ptr, n2 * sizeof(cd), cudaMemcpyDeviceToHost, stream_), "download");
+    check_cuda(cudaStreamSynchronize(stream_), "download");
+  };
+  download(iterations > 0 ? t_iter.ptr + (iterations - 1) * n2 : e, out.transmitted);
+  if (out.reflected) {
+    if (iterations > 0)
+      download(r_iter.ptr + (iterations - 1) * n2, out.reflected);
+    else
+      std::memset(static_cast<void*>(out.reflected), 0, n2 * sizeof(cd));
+  }
+  for (int it = 0; it < iterations; ++it) {
+    if (out.transmitted_iter) download(t_iter.ptr + it * n2, out.transmitted_iter + it * n2);
+    if (out.reflected_iter) download(r_iter.ptr + it * n2, out.reflected_iter + it * n2);
+  }
+  for (std::size_t i = 0; i < nkeep; ++i) {
+    if (out.forward) download(kept_f.ptr + i * n2, out.forward + i * n2);
+    if (out.backward && iterations > 0) download(kept_b.ptr + i * n2, out.backward + i * n2);
+  }
+  out.stored_values = iterations > 0 ? 2 * iface_total_ : 0;
+  check_cuda(cudaStreamSynchronize(stream_), "synchronize");
+}
+
+template <typename T>
+std::size_t PlaneSolver<T>::device_bytes() const {
+  std::size_t b = 0;
+  for (auto& kv : tables_) b += kv.second.bytes();
+  for (const auto* d : {&input_, &e_, &next_, &spec_, &xbuf_, &work_, &src_fwd_, &src_bwd_, &pot_,
+                        &born_fwd_, &born_bwd_, &w3_, &t3_, &sources_})
+    b += d->bytes();
+  return b + pid_pool_.bytes() + iface_pool_.bytes() + rowoff_pool_.bytes() + mask_.bytes();
+}
+
+}  // namespace
+
+std::unique_ptr<Solver> make_plane_solver(SolverInput in, int precision) {
+  if (precision == 64) return std::make_unique<PlaneSolver<double>>(std::move(in));
+  if (precision == 32) return std::make_unique<PlaneSolver<float>>(std::move(in));
+  throw invalid_argument("precision must be 64 or 32");
+}
+
+namespace {
+__global__ void k_interface(int reflection, const double* kx, const double* ky, long long n,
+                            cd n_in, cd n_out, double k0, cd* out) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  cd m[3];
+  interface_matrix(reflection != 0, kx[i], ky[i], n_in, n_out, k0, m);
+  out[4 * i] = m[0];
+  out[4 * i + 1] = m[1];
+  out[4 * i + 2] = m[1];
+  out[4 * i + 3] = m[2];
+}
+
+__global__ void k_kz(cd index, double k0, const double* kp2, long long n, cd* out) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i < n) out[i] = kz_of(index, k0, kp2[i]);
+}
+}  // namespace
+
+void interface_matrices(int reflection, const double* kx, const double* ky, std::size_t n,
+                        cd n_in, cd n_out, double k0, cd* out) {
+  if (n == 0) return;
+  DevBuf<double> dkx(n), dky(n);
+  DevBuf<cd> dout(4 * n);
+  check_cuda(cudaMemcpy(dkx.ptr, kx, n * sizeof(double), cudaMemcpyHostToDevice), "upload");
+  check_cuda(cudaMemcpy(dky.ptr, ky, n * sizeof(double), cudaMemcpyHostToDevice), "upload");
+  k_interface<<<ceil_div(n, kThreads), kThreads>>>(reflection, dkx.ptr, dky.ptr,
+                                                    static_cast<long long>(n), n_in, n_out, k0, dout.ptr);
+  check_cuda(cudaGetLastError(), "k_interface");
+  check_cuda(cudaMemcpy(out, dout.ptr, 4 * n * sizeof(cd), cudaMemcpyDeviceToHost), "download");
+}
+
+void longitudinal_wavenumbers(cd index, double k0, const double* kp2, std::size_t n, cd* out) {
+  if (n == 0) return;
+  DevBuf<double> d(n);
+  DevBuf<cd> o(n);
+  check_cuda(cudaMemcpy(d.ptr, kp2, n * sizeof(double), cudaMemcpyHostToDevice), "upload");
+  k_kz<<<ceil_div(n, kThreads), kThreads>>>(index, k0, d.ptr, static_cast<long long>(n), o.ptr);
+  check_cuda(cudaGetLastError(), "k_kz");
+  check_cuda(cudaMemcpy(out, o.ptr, n * sizeof(cd), cudaMemcpyDeviceToHost), "download");
+}
+
+int device_count() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+}  // namespace bwpm

@@ -1,0 +1,84 @@
+/* C ABI of bwpm_b200: the B200-native slab-stepping core of BWPM (libbwpm_b200.so).
+ *
+ * Drop-in boundary for the reference's compiled module `bwpm._core` (pybind11,
+ * cpp/python/bindings.cpp:122-180). Every entry point takes plain pointers and sizes; complex
+ * values are interleaved (re, im) doubles (numpy complex128 memory). All entry points return a
+ * status: BWPM_OK, BWPM_EINVAL (the reference raises std::invalid_argument -> ValueError) or
+ * BWPM_ERUNTIME (std::runtime_error -> RuntimeError: CUDA failure, GMRES non-convergence).
+ * bwpm_last_error() gives the message of the last failure on the calling thread.
+ */
+#ifndef BWPM_B200_H
+#define BWPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BWPM_OK 0
+#define BWPM_EINVAL 1
+#define BWPM_ERUNTIME 2
+
+typedef struct bwpm_solver bwpm_solver;
+
+/* Message of the last failed call on this thread; returns its full length. */
+size_t bwpm_last_error(char* buf, size_t len);
+
+/* Library version string. */
+const char* bwpm_version(void);
+
+/* Number of usable CUDA devices, 0 without a driver.
+ * Replaces bwpm._core.cuda_device_count (cpp/python/bindings.cpp:157, cpp/src/solver_cuda.cu:357-364). */
+int bwpm_cuda_device_count(void);
+
+/* Transmission (reflection = 0) or reflection (reflection = 1) matrices of a plane interface
+ * without propagation factor at n points (k_x[i], k_y[i]); out: n·2·2 complex (row-major 2×2).
+ * Replaces bwpm._core.transmission_matrix / reflection_matrix
+ * (cpp/python/bindings.cpp:124-137, cpp/src/interface.cpp:30-52). Computed in FP64 on device 0. */
+int bwpm_interface_matrices(int reflection, const double* k_x, const double* k_y, size_t n,
+                            double index_in_re, double index_in_im, double index_out_re,
+                            double index_out_im, double k0, double* out);
+
+/* k_z = sqrt(ñ²k₀² − k⊥²) with the grazing rule at n values of k⊥²; out: n complex.
+ * Replaces bwpm._core.longitudinal_wavenumber (cpp/python/bindings.cpp:178-179,
+ * cpp/src/interface.cpp:8-18). */
+int bwpm_longitudinal_wavenumber(double index_re, double index_im, double k0,
+                                 const double* k_perp_sq, size_t n, double* out);
+
+/* Creates a solver on `device`. indices: m complex; labels: nz·ny·nx int32 (C order);
+ * mask: ny·nx doubles or NULL; fluctuation: nz·ny·nx complex or NULL. precision: 64 for the
+ * complex128 drop-in path, 32 for complex64 fields with FP64 operator tables. gmres_tol: GMRES
+ * tolerance of the Born step (the reference uses 1e-12).
+ * Replaces bwpm._core.CudaSolver(ny, nx, dy, dx, dz, k0, indices, labels, index_before, mask,
+ * device, fluctuation) (cpp/python/bindings.cpp:158-171, cpp/src/solver_cuda.cu:643-719). */
+int bwpm_solver_create(size_t ny, size_t nx, double dy, double dx, double dz, double k0,
+                       const double* indices, size_t m, const int32_t* labels, size_t nz,
+                       double index_before_re, double index_before_im, const double* mask,
+                       int device, const double* fluctuation, int precision, double gmres_tol,
+                       bwpm_solver** out);
+
+/* Runs `iterations` bidirectional iterations (0: forward FPWPM only) on field (ny·nx·2 complex).
+ * keep: nkeep sorted unique plane numbers ≤ nz. Outputs (complex, caller-allocated, may be
+ * NULL): transmitted and reflected (ny·nx·2 each), transmitted_iter/reflected_iter
+ * (iterations planes), forward/backward (nkeep planes; backward only for iterations > 0).
+ * Replaces CudaSolver.run(field, iterations, keep) -> dict
+ * (cpp/python/bindings.cpp:61-86, cpp/src/solver_cuda.cu:729-853). */
+int bwpm_solver_run(bwpm_solver* s, const double* field, int iterations, const int64_t* keep,
+                    size_t nkeep, double* transmitted, double* reflected,
+                    double* transmitted_iter, double* reflected_iter, double* forward,
+                    double* backward, int64_t* stored_values);
+
+/* Device memory held by the solver, kernels it launched so far, GMRES operator applications. */
+int bwpm_solver_stats(const bwpm_solver* s, int64_t* device_bytes, int64_t* kernel_launches,
+                      int64_t* gmres_applies);
+
+/* Releases the solver (CudaSolver destructor, cpp/src/solver_cuda.cu:721-727). */
+void bwpm_solver_destroy(bwpm_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BWPM_B200_H */
