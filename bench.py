@@ -1,0 +1,364 @@
+"""Benchmark: batched complex64 2D BWPM solves per second on one B200 (or N replicas).
+
+Workload (seeded, synthetic): 256 tilted-slab 2D solves of uneven size (ny 256-8192 including
+3·2^k, nz 100-2000 slabs, λ 0.4-1.0 µm, 0-30° incidence, n 1.4-1.8, 0-8° tilted front face,
+absorbing mask, TE/TM alternating, 6 bidirectional iterations); bwpm_b200.workloads.batch2d.
+A step is one solve of the whole batch. `value` is solves/s with inputs resident on the device;
+`e2e` is the same through the public batch API with host copies of the incident fields and of
+the transmitted/reflected results inside the timed region.
+
+Beside it: p50/p99 per-solve device latency, the plain per-solve FP64 GPU path (the drop-in
+CudaSolver) on a seeded sample of the same batch with the relative L2 error of the batched
+complex64 results against it, the roofline of the resident kernel, and the reference CPU core
+(oracle/_ref, built from the reference's own sources) on a bounded sample, all host cores.
+
+--impl reference: times the reference CPU implementation on the same workload and metric.
+Multi-GPU (torchrun): replicas only, every rank solves its own copy of the batch.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "solves/s (batched complex64 2D BWPM, 256 uneven solves, 6 iterations)"
+WORKLOAD = ("batched-2d: 256 seeded tilted-slab solves, ny 256-8192 incl. 3*2^k, nz 100-2000, "
+            "lambda 0.4-1.0 um, 0-30 deg incidence, n 1.4-1.8, 0-8 deg tilt, mask, TE/TM, "
+            "6 iterations")
+COUNT, SEED = 256, 4
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs × FP32 lanes × FMA × max clock
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from datetime import timedelta
+
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+    return dist, rank, ws
+
+
+def _max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._loop, daemon=True)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:  # noqa: BLE001 - sampling is best effort
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---- CPU reference (oracle/_ref: the reference's own C++ CPU core) ---------------------------
+
+def _cpu_solve(args):
+    """One solve on the reference CPU core (1 thread) or, without it, the numpy oracle port."""
+    prm, kind = args
+    from bwpm_b200 import workloads
+
+    p = workloads.tilted_slab2d_from(prm)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        import importlib.util
+
+        so = sorted((ROOT / "oracle" / "_ref").glob("_core*.so"))[0]
+        spec = importlib.util.spec_from_file_location("_core", so)
+        core = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(core)
+        core.Solver(*p.core_args(), 1).run(p.field, p.iterations, [])
+    else:
+        from oracle import port
+
+        port.Solver(*p.core_args()).run(p.field, p.iterations)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(params: list[dict], budget_s: float = 20.0) -> dict:
+    """Reference CPU throughput on a bounded seeded sample of the batch, all host cores.
+
+    Runs a seeded random sample of the batch's instances as single-threaded solves in a pool of
+    one process per core (no GPU work meanwhile) and reports cores × solves / Σ solve time."""
+    import multiprocessing as mp
+
+    kind = "reference" if sorted((ROOT / "oracle" / "_ref").glob("_core*.so")) else "port"
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(123)
+    order = rng.permutation(len(params))
+    # estimated single-thread cost: ≈ 1.2e-8 s per point·log2(N) per slab-pass (reference core)
+    est = [1.2e-8 * p["ny"] * np.log2(p["ny"]) * p["nz"] * 2 * p["iterations"] * 2 for p in params]
+    sample, tot = [], 0.0
+    for i in order:
+        if tot > budget_s * cores and len(sample) >= min(cores, 4):
+            break
+        sample.append(int(i))
+        tot += est[i]
+        if len(sample) >= 4 * cores:
+            break
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(min(cores, len(sample))) as pool:
+        times = pool.map(_cpu_solve, [(params[i], kind) for i in sample])
+    wall = time.perf_counter() - t0
+    per_solve = float(np.mean(times))
+    return {"value": cores / per_solve, "unit": "solves/s", "cores": cores, "kind": kind,
+            "sample": f"{len(sample)} seeded random instances of the batch (indices {sample[:8]}...), "
+                      f"1 thread each in {min(cores, len(sample))} processes; "
+                      f"throughput = cores / mean solve time ({per_solve:.2f} s); wall {wall:.1f} s"}
+
+
+def run_reference(args) -> None:
+    dist, rank, ws = _dist_for_reference()
+    if rank != 0:
+        return
+    params = _params()
+    vals = []
+    cb = None
+    for _ in range(args.warmup):
+        pass  # the CPU core has no warm-up state worth a step of its own
+    for _ in range(args.steps):
+        cb = cpu_baseline(params, budget_s=args.cpu_budget)
+        vals.append(cb["value"])
+    v = float(np.median(vals))
+    line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": COUNT / v * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "global_batch": COUNT, "seq_len": None,
+                       "parallelism": "cpu"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cb["cores"],
+                             "kind": cb["kind"], "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _dist_for_reference():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    return None, rank, ws
+
+
+def _params():
+    from bwpm_b200 import workloads
+
+    return workloads.batch2d_params(COUNT, SEED)
+
+
+# ---- our arm ----------------------------------------------------------------------------------
+
+def run_ours(args) -> None:
+    dist, rank, ws = _dist()
+    device = int(os.environ.get("LOCAL_RANK", "0")) if dist else 0
+    from bwpm_b200 import _core, workloads
+    from bwpm_b200.batch import Batch2D, flush_l2, host_register, host_unregister
+    from bwpm_b200.model import Grid2D, power_flux
+
+    params = _params()
+    t_setup = time.perf_counter()
+    b = Batch2D(device)
+    fields = []
+    for prm in params:
+        p = workloads.tilted_slab2d_from(prm)
+        b.add_problem(p)
+        fields.append(p.field[:, 0, :].copy())
+        del p
+    b.prepare()
+    setup_s = time.perf_counter() - t_setup
+    stats = b.stats()
+    work = b.work()
+    packed_in = np.ascontiguousarray(np.concatenate([f.ravel() for f in fields]))
+    packed_out = np.empty(2 * packed_in.size, dtype=np.complex128)
+    host_register(packed_in)
+    host_register(packed_out)
+    for _ in range(args.warmup):
+        b.run()
+    _barrier(dist)
+    times = []
+    with Clocks(device) as clk:
+        for _ in range(args.steps):
+            flush_l2(device)
+            _barrier(dist)
+            times.append(b.run())
+    clocks = clk.summary()
+    step_ms = _max_over_ranks(dist, float(np.sum(times))) / args.steps
+    lat = np.array([b.result(i)["latency_ms"] for i in range(COUNT)])
+    # end to end through the public API: H2D of incident fields, solve, D2H of results
+    e2e_times = []
+    for _ in range(max(1, args.warmup // 2)):
+        b.solve_packed(packed_in, packed_out)
+    for _ in range(args.steps):
+        flush_l2(device)
+        e2e_times.append(b.solve_packed(packed_in, packed_out))
+    e2e_ms = _max_over_ranks(dist, float(np.mean(e2e_times)))
+    host_unregister(packed_in)
+    host_unregister(packed_out)
+    if rank != 0:
+        _barrier(dist)
+        return
+    value = ws * COUNT / (step_ms * 1e-3)
+    # plain per-solve FP64 GPU path (drop-in CudaSolver) on a seeded sample; L2 error of the
+    # batched complex64 results against it
+    rng = np.random.default_rng(7)
+    sample = [int(i) for i in rng.permutation(COUNT)[: args.fp64_sample]]
+    fp64_t, errs, eps_err = [], [], []
+    for i in sample:
+        p = workloads.tilted_slab2d_from(params[i])
+        s = _core.CudaSolver(*p.core_args(), device)
+        t0 = time.perf_counter()
+        r64 = s.run(p.field, p.iterations, [])
+        fp64_t.append(time.perf_counter() - t0)
+        r32 = b.result(i)
+        for key in ("transmitted", "reflected"):
+            ref = r64[key][:, 0]
+            errs.append(float(np.linalg.norm(r32[key] - ref) / max(np.linalg.norm(ref), 1e-300)))
+        g = Grid2D(p.ny, p.dy, p.dz, prm_wl(params[i]))
+        p_in = power_flux(p.field[:, 0], g, p.index_before)
+        last = complex(p.indices[int(p.labels[-1, p.ny // 2, 0])])
+        for k in range(p.iterations):
+            pt = power_flux(r64["transmitted_iter"][k][:, 0], g, last)
+            pr = power_flux(r64["reflected_iter"][k][:, 0], g, p.index_before, direction=-1)
+            # energy balance error relative to the largest flux involved
+            eps_err.append(abs(r32["energy_residual"][k] - (1.0 - (pt + pr) / p_in))
+                           / max(1.0, (pt + pr) / p_in))
+        del s
+    mean_cost = np.mean([prm["ny"] * np.log2(prm["ny"]) * prm["nz"] for prm in params])
+    samp_cost = np.mean([params[i]["ny"] * np.log2(params[i]["ny"]) * params[i]["nz"] for i in sample])
+    fp64_rate = 1.0 / (np.mean(fp64_t) * mean_cost / samp_cost)
+    # roofline of the resident kernel: algorithmic FLOPs per launch ÷ launch time
+    kern_s = step_ms * 1e-3
+    achieved = work["flops"] / kern_s / 1e12
+    hbm_peak = _peak("hbm_gbs")
+    cb = cpu_baseline(params, budget_s=args.cpu_budget) if not args.no_cpu else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "global_batch": COUNT * ws, "seq_len": None,
+                   "parallelism": f"replicas{ws}", "l2": "flushed (512 MB write) before each timed step",
+                   "work_items": stats["work_items"], "classes": stats["classes"]},
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "fp64_plain": {"value": fp64_rate, "unit": "solves/s", "sample": len(sample),
+                       "note": "per-solve FP64 CudaSolver (drop-in path), mean sample time scaled "
+                               "to the batch's mean N·log2N·nz",
+                       "speedup_batched_c64": value / ws / fp64_rate},
+        "l2_err_max": float(np.max(errs)),
+        "eps_err_max": float(np.max(eps_err)) if eps_err else None,
+        "eps_err_note": "|eps_c64 - eps_fp64| / max(1, (P_R + P_T)/P_in) over the sample's iterations",
+        "e2e": {"value": ws * COUNT / (e2e_ms * 1e-3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(packed_in.nbytes), "d2h_bytes_per_step": int(packed_out.nbytes)},
+        "gpu_launches": int(stats["classes"]) * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS,
+                     "unit": "TFLOP/s", "frac": achieved / FP32_NOMINAL_TFLOPS,
+                     "traffic": None,
+                     "note": "shared-memory FFT: SIMT FP32 and shared-memory bound, no tensor "
+                             "cores (FFT is not a dense contraction); peak = nominal FP32 "
+                             "(no measured FP32 peak in MEASURED_PEAKS.json)",
+                     "hbm": {"achieved": work["bytes"] / kern_s / 1e9, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": work["bytes"] / kern_s / 1e9 / hbm_peak}},
+        "cpu_baseline": cb,
+        "clocks": clocks,
+        "setup_s": setup_s,
+        "device_bytes": stats["device_bytes"],
+    }
+    print(json.dumps(line), flush=True)
+    _barrier(dist)
+
+
+def prm_wl(prm: dict) -> float:
+    return float(prm["wl"])
+
+
+def _peak(key: str) -> float:
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())[key])
+    except Exception:  # noqa: BLE001
+        return {"hbm_gbs": 6650.0}.get(key, float("nan"))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fp64-sample", type=int, default=6)
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="target CPU seconds per core")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -41,6 +41,18 @@ SIGNATURES: dict[str, tuple] = {
     "bwpm_solver_run": (_i, [_p, _p, _i, _p, _sz, _p, _p, _p, _p, _p, _p, _i64p]),
     "bwpm_solver_stats": (_i, [_p, _i64p, _i64p, _i64p]),
     "bwpm_solver_destroy": (None, [_p]),
+    "bwpm_batch_create": (_i, [_i, ctypes.POINTER(_p)]),
+    "bwpm_batch_add": (_i, [_p, _sz, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _p, _i, _i64p]),
+    "bwpm_batch_prepare": (_i, [_p]),
+    "bwpm_batch_run": (_i, [_p, ctypes.POINTER(ctypes.c_float)]),
+    "bwpm_batch_solve_packed": (_i, [_p, _p, _p, ctypes.POINTER(ctypes.c_float)]),
+    "bwpm_batch_result": (_i, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, _p]),
+    "bwpm_batch_stats": (_i, [_p, _i64p, _i64p, _i64p, _i64p, _i64p]),
+    "bwpm_batch_work": (_i, [_p, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d)]),
+    "bwpm_batch_destroy": (None, [_p]),
+    "bwpm_flush_l2": (_i, [_i, _sz]),
+    "bwpm_host_register": (_i, [_p, _sz]),
+    "bwpm_host_unregister": (_i, [_p]),
 }
 
 

@@ -1,0 +1,728 @@
+// Batched resident 2D engine: host preparation, size classes and launches.
+//
+// Preparation turns each solve's int32 labels (nz, ny) into per-step records (pairs, uint8
+// pair-id planes deduplicated within the solve, interface pixel lists, pass lists of the four
+// table-1 kinds; cpp/src/solver.cpp:384-417, :444-460) and registers one operator table per
+// (kind, ñ_r, ñ_s) and solve, built on the device in FP64 and stored as complex64 for E_x (m00)
+// and E_y (m11). Work items (solve, component) are grouped into size classes by CTA width; each
+// class is one persistent kernel on its own stream, all launched together.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <stdexcept>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+
+#include "batch2d.hpp"
+#include "devbuf.hpp"
+#include "interface.cuh"
+#include "plan.hpp"
+#include "resident2d.cuh"
+
+namespace bwpm {
+namespace {
+
+constexpr int kClassThreads[] = {128, 256, 512, 1024};
+constexpr int kNumClasses = 4;
+
+// Operator table job: M/N of `kind` for (ñ_r, ñ_s), entry m00 (E_x) at out[0..2N) and m11 (E_y)
+// at out[2N..4N), each as N hi values then N lo values with M/N = hi + lo (built in FP64; the
+// inverse transform's 1/N is folded in).
+struct TableJob {
+  cf* out;
+  cd nr, ns;
+  double dy, k0, dz;
+  int n, kind;
+};
+
+__global__ void k_table_jobs(const TableJob* jobs) {
+  const TableJob j = jobs[blockIdx.y];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= j.n) return;
+  const double ky = fftfreq(q, j.n, j.dy);
+  cd m[3];
+  operator_matrix(j.kind, 0.0, ky, j.nr, j.ns, j.k0, j.dz, m);
+  const double inv_n = 1.0 / static_cast<double>(j.n);
+  for (int c = 0; c < 2; ++c) {
+    const cd v = m[2 * c] * inv_n;
+    const cf hi = cast<float>(v);
+    j.out[2 * c * j.n + q] = hi;
+    j.out[(2 * c + 1) * j.n + q] = cf{static_cast<float>(v.re - hi.re), static_cast<float>(v.im - hi.im)};
+  }
+}
+
+// Flux weights Re k_z·(1 + [E_y] k_y²/|k_z|²)·dy/ny of a medium (src/bwpm/fpwpm.py:205-216).
+struct WeightJob {
+  double* out;
+  cd index;
+  double dy, k0;
+  int n, comp;
+};
+
+__global__ void k_weight_jobs(const WeightJob* jobs) {
+  const WeightJob j = jobs[blockIdx.y];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= j.n) return;
+  const double ky = fftfreq(q, j.n, j.dy);
+  const cd kz = kz_of(j.index, j.k0, ky * ky);
+  double w = kz.re * j.dy / j.n;
+  if (j.comp == 1) w *= 1.0 + ky * ky / (kz.re * kz.re + kz.im * kz.im);
+  j.out[q] = w;
+}
+
+// Scatter packed complex128 inputs (ny, 2) per solve into the per-item complex64 lines.
+struct ItemIo {
+  long long packed;  // offset of the solve's (ny, 2) block in the packed arrays
+  cf* line_in;
+  const cf* line_t;
+  const cf* line_r;
+  int n, comp;
+};
+
+__global__ void k_unpack_inputs(const ItemIo* io, const cd* packed) {
+  const ItemIo j = io[blockIdx.y];
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < j.n; q += gridDim.x * blockDim.x)
+    j.line_in[q] = cast<float>(packed[j.packed + 2 * q + j.comp]);
+}
+
+__global__ void k_pack_outputs(const ItemIo* io, cd* out) {
+  // out: per solve (transmitted (ny, 2), reflected (ny, 2)); components without an item stay 0
+  const ItemIo j = io[blockIdx.y];
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < j.n; q += gridDim.x * blockDim.x) {
+    out[2 * j.packed + 2 * q + j.comp] = cast<double>(j.line_t[q]);
+    out[2 * j.packed + 2 * j.n + 2 * q + j.comp] = cast<double>(j.line_r[q]);
+  }
+}
+
+struct HostSolve {
+  Solve2D in;
+  // offsets into the pools
+  long long step_base = 0, pass_base = 0, pid_base = 0, iface_base = 0, table_base = 0;
+  long long iface_count = 0;
+  long long packed = 0;
+  std::vector<R2Step> steps;
+  std::vector<R2Pass> passes;
+  std::vector<std::uint8_t> pids;
+  std::vector<int> iface;
+  std::vector<std::tuple<int, cd, cd>> tables;  // (kind, ñ_r, ñ_s) per table slot
+  int items[2] = {-1, -1};
+};
+
+struct Item {
+  int solve, comp, cls, n;
+  double cost;
+};
+
+class Batch2DImpl final : public Batch2D {
+ public:
+  explicit Batch2DImpl(int device) : device_(device) {
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    for (auto& s : streams_) check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaStreamCreateWithFlags(&main_, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaEventCreate(&ev0_), "event");
+    check_cuda(cudaEventCreate(&ev1_), "event");
+    for (auto& e : class_done_) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    cudaDeviceProp prop{};
+    check_cuda(cudaGetDeviceProperties(&prop, device), "props");
+    sms_ = prop.multiProcessorCount;
+  }
+  ~Batch2DImpl() override {
+    for (auto& s : streams_) cudaStreamDestroy(s);
+    cudaStreamDestroy(main_);
+    cudaEventDestroy(ev0_);
+    cudaEventDestroy(ev1_);
+    for (auto& e : class_done_) cudaEventDestroy(e);
+  }
+
+  std::int64_t add(Solve2D s) override {
+    if (prepared_) throw invalid_argument("batch already prepared");
+    validate(s);
+    HostSolve h;
+    h.in = std::move(s);
+    solves_.push_back(std::move(h));
+    return static_cast<std::int64_t>(solves_.size()) - 1;
+  }
+
+  void prepare() override;
+  float run() override;
+  float solve_packed(const cd* fields, cd* out) override;
+  void result(std::int64_t id, Solve2DResult& r) override;
+  std::size_t device_bytes() const override { return bytes_; }
+  std::int64_t kernel_launches() const override { return launches_; }
+  int work_items() const override { return static_cast<int>(items_.size()); }
+  int classes() const override {
+    int c = 0;
+    for (int k = 0; k < kNumClasses; ++k) c += class_count_[k] > 0;
+    return c;
+  }
+  std::size_t packed_inputs() const override { return static_cast<std::size_t>(packed_total_); }
+  void work(double& transforms, double& flops, double& bytes) const override {
+    transforms = work_transforms_;
+    flops = work_flops_;
+    bytes = work_bytes_;
+  }
+
+ private:
+  static void validate(const Solve2D& s) {
+    if (s.ny < 2) throw invalid_argument("ny must be >= 2");
+    if (s.nz < 1) throw invalid_argument("nz must be >= 1");
+    if (s.labels.size() != static_cast<std::size_t>(s.nz) * s.ny)
+      throw invalid_argument("labels must have shape (nz, ny)");
+    if (!s.mask.empty() && s.mask.size() != static_cast<std::size_t>(s.ny))
+      throw invalid_argument("mask must have shape (ny,)");
+    if (s.field.size() != static_cast<std::size_t>(2 * s.ny)) throw invalid_argument("field must have shape (ny, 2)");
+    if (s.iterations < 0) throw invalid_argument("iterations must be >= 0");
+    for (auto l : s.labels)
+      if (l < 0 || static_cast<std::size_t>(l) >= s.indices.size())
+        throw invalid_argument("labels must index into `indices`");
+    if (s.indices.size() > 255) throw invalid_argument("at most 255 materials per 2D solve");
+    if (3 * static_cast<std::size_t>(s.ny) * sizeof(cf) > 220 * 1024)
+      throw invalid_argument("ny too large for the resident 2D engine (max 9216)");
+  }
+  void prepare_solve(HostSolve& h);
+  void launch_classes(cudaStream_t origin);
+  template <typename K, typename... A>
+  void launch(K kernel, dim3 grid, dim3 block, std::size_t smem, cudaStream_t s, A... args) {
+    kernel<<<grid, block, smem, s>>>(args...);
+    check_cuda(cudaGetLastError(), "kernel launch");
+    ++launches_;
+  }
+
+  int device_;
+  int sms_ = 148;
+  bool prepared_ = false;
+  std::vector<HostSolve> solves_;
+  std::vector<Item> items_;
+  cudaStream_t streams_[kNumClasses] = {};
+  cudaStream_t main_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t class_done_[kNumClasses] = {};
+  int class_count_[kNumClasses] = {};
+  int class_first_[kNumClasses] = {};
+  int class_maxn_[kNumClasses] = {};
+  int class_grid_[kNumClasses] = {};
+  // device pools
+  DevBuf<R2Step> d_steps_;
+  DevBuf<R2Pass> d_passes_;
+  DevBuf<std::uint8_t> d_pids_;
+  DevBuf<int> d_iface_;
+  DevBuf<cf> d_tables_, d_lines_, d_src_;
+  DevBuf<Tw<float>> d_twiddles_;
+  DevBuf<FftPlan> d_plans_;
+  DevBuf<float> d_mask_;
+  DevBuf<double> d_weights_, d_energy_;
+  DevBuf<long long> d_clock_;
+  DevBuf<R2Item> d_items_;
+  DevBuf<int> d_queue_;
+  DevBuf<ItemIo> d_io_;
+  DevBuf<cd> d_packed_in_, d_packed_out_;
+  std::vector<R2Item> h_items_;
+  std::vector<long long> item_energy_off_;
+  long long packed_total_ = 0;
+  std::size_t bytes_ = 0;
+  std::int64_t launches_ = 0;
+  double work_transforms_ = 0, work_flops_ = 0, work_bytes_ = 0;
+};
+
+void Batch2DImpl::prepare_solve(HostSolve& h) {
+  const Solve2D& s = h.in;
+  const int n = s.ny;
+  auto index_of = [&](int l) { return l < 0 ? s.index_before : s.indices[static_cast<std::size_t>(l)]; };
+  auto same = [](cd a, cd b) { return a.re == b.re && a.im == b.im; };
+  std::map<std::tuple<int, double, double, double, double>, int> slot;
+  auto table = [&](int kind, cd nr, cd ns) -> long long {
+    auto key = std::make_tuple(kind, nr.re, nr.im, ns.re, ns.im);
+    auto it = slot.find(key);
+    int id;
+    if (it == slot.end()) {
+      id = static_cast<int>(h.tables.size());
+      slot.emplace(key, id);
+      h.tables.emplace_back(kind, nr, ns);
+    } else {
+      id = it->second;
+    }
+    return static_cast<long long>(id) * 4 * n;
+  };
+  std::unordered_map<std::uint64_t, std::vector<long long>> seen;
+  std::vector<std::int32_t> before(n, -1);
+  std::vector<std::uint8_t> pid(n);
+  std::vector<std::pair<int, int>> pairs;
+  const bool refl = s.iterations > 0;
+  h.steps.resize(s.nz);
+  for (int p = 0; p < s.nz; ++p) {
+    const std::int32_t* a = p == 0 ? before.data() : s.labels.data() + static_cast<std::size_t>(p - 1) * n;
+    const std::int32_t* b = s.labels.data() + static_cast<std::size_t>(p) * n;
+    pairs.clear();
+    for (int q = 0; q < n; ++q) {
+      const std::pair<int, int> pr{a[q], b[q]};
+      if (std::find(pairs.begin(), pairs.end(), pr) == pairs.end()) pairs.push_back(pr);
+    }
+    std::sort(pairs.begin(), pairs.end());
+    R2Step st{};
+    st.pid = -1;
+    if (pairs.size() > 1) {
+      std::uint64_t hash = 1469598103934665603ULL;
+      for (int q = 0; q < n; ++q) {
+        const std::pair<int, int> pr{a[q], b[q]};
+        pid[q] = static_cast<std::uint8_t>(std::lower_bound(pairs.begin(), pairs.end(), pr) - pairs.begin());
+        hash = (hash ^ pid[q]) * 1099511628211ULL;
+      }
+      long long found = -1;
+      for (long long off : seen[hash])
+        if (std::memcmp(h.pids.data() + off, pid.data(), n) == 0) {
+          found = off;
+          break;
+        }
+      if (found < 0) {
+        found = static_cast<long long>(h.pids.size());
+        h.pids.insert(h.pids.end(), pid.begin(), pid.end());
+        seen[hash].push_back(found);
+      }
+      st.pid = found;
+    }
+    st.iface = static_cast<long long>(h.iface.size());
+    for (int q = 0; q < n; ++q)
+      if (!same(index_of(a[q]), index_of(b[q]))) h.iface.push_back(q);
+    st.niface = static_cast<int>(h.iface.size() - st.iface);
+    // forward passes: T for every pair, then R where the indices differ (cpp/src/solver.cpp:396-397)
+    st.fwd_off = static_cast<int>(h.passes.size());
+    for (std::size_t i = 0; i < pairs.size(); ++i)
+      h.passes.push_back({table(kFwdT, index_of(pairs[i].first), index_of(pairs[i].second)), static_cast<int>(i), 0});
+    st.fwd_t = static_cast<int>(pairs.size());
+    st.fwd_r = 0;
+    if (refl)
+      for (std::size_t i = 0; i < pairs.size(); ++i) {
+        const cd nr = index_of(pairs[i].first), ns = index_of(pairs[i].second);
+        if (same(nr, ns)) continue;
+        h.passes.push_back({table(kFwdR, nr, ns), static_cast<int>(i), 1});
+        ++st.fwd_r;
+      }
+    // backward step from plane p + 1 to plane p: roles swapped
+    st.bwd_off = static_cast<int>(h.passes.size());
+    st.bwd_t = st.bwd_r = 0;
+    if (refl) {
+      for (std::size_t i = 0; i < pairs.size(); ++i) {
+        h.passes.push_back({table(kBwdT, index_of(pairs[i].second), index_of(pairs[i].first)), static_cast<int>(i), 0});
+        ++st.bwd_t;
+      }
+      for (std::size_t i = 0; i < pairs.size(); ++i) {
+        const cd nr = index_of(pairs[i].second), ns = index_of(pairs[i].first);
+        if (same(nr, ns)) continue;
+        h.passes.push_back({table(kBwdR, nr, ns), static_cast<int>(i), 1});
+        ++st.bwd_r;
+      }
+    }
+    h.steps[p] = st;
+  }
+  h.iface_count = static_cast<long long>(h.iface.size());
+}
+
+void Batch2DImpl::prepare() {
+  if (prepared_) return;
+  if (solves_.empty()) throw invalid_argument("empty batch");
+  check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+  // host preparation, parallel over solves
+  {
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    std::atomic<std::size_t> next{0};
+    std::vector<std::exception_ptr> errs(hw);
+    for (unsigned t = 0; t < hw; ++t)
+      pool.emplace_back([&, t] {
+        try {
+          for (std::size_t i = next++; i < solves_.size(); i = next++) prepare_solve(solves_[i]);
+        } catch (...) {
+          errs[t] = std::current_exception();
+        }
+      });
+    for (auto& th : pool) th.join();
+    for (auto& e : errs)
+      if (e) std::rethrow_exception(e);
+  }
+  // plans per distinct length, twiddle pool
+  std::map<int, int> plan_of;
+  std::vector<FftPlan> plans;
+  std::vector<Tw<float>> tw;
+  for (auto& h : solves_) {
+    const int n = h.in.ny;
+    if (plan_of.count(n)) continue;
+    HostPlan hp = make_plan(n);
+    const int base = static_cast<int>(tw.size());
+    for (auto& t : twiddles_for<float>(hp)) tw.push_back(t);
+    for (int s = 0; s < hp.plan.nstages; ++s) hp.plan.twoff[s] += base;
+    hp.plan.rootoff += base;
+    plan_of[n] = static_cast<int>(plans.size());
+    plans.push_back(hp.plan);
+  }
+  // pool offsets
+  long long nsteps = 0, npass = 0, npid = 0, niface = 0, ntab = 0, nlines = 0, nsrc = 0, nmask = 0,
+            nweights = 0, nenergy = 0;
+  for (auto& h : solves_) {
+    h.step_base = nsteps;
+    h.pass_base = npass;
+    h.pid_base = npid;
+    h.iface_base = niface;
+    h.table_base = ntab;
+    h.packed = packed_total_;
+    nsteps += h.in.nz;
+    npass += static_cast<long long>(h.passes.size());
+    npid += static_cast<long long>(h.pids.size());
+    niface += h.iface_count;
+    ntab += static_cast<long long>(h.tables.size()) * 4 * h.in.ny;
+    packed_total_ += 2LL * h.in.ny;
+    if (!h.in.mask.empty()) nmask += 2LL * h.in.ny;
+  }
+  // work items: (solve, component) with a non-zero input component
+  for (std::size_t i = 0; i < solves_.size(); ++i) {
+    HostSolve& h = solves_[i];
+    const int n = h.in.ny;
+    for (int c = 0; c < 2; ++c) {
+      bool any = false;
+      for (int q = 0; q < n && !any; ++q) any = h.in.field[2 * q + c].re != 0.0 || h.in.field[2 * q + c].im != 0.0;
+      if (!any) continue;
+      int cls = 0;
+      const int want = threads_needed(plans[plan_of[n]], 1, kR2Ept);
+      if (want > kClassThreads[kNumClasses - 1])
+        throw invalid_argument("ny = " + std::to_string(n) + " needs more than 1024 threads in the resident 2D engine");
+      while (cls < kNumClasses - 1 && kClassThreads[cls] < want) ++cls;
+      double passes = 0;
+      for (auto& st : h.steps) passes += 2 + st.fwd_t + st.fwd_r + st.bwd_t + st.bwd_r;
+      const double cost = std::max(1, h.in.iterations) * passes * n * std::log2(std::max(2, n));
+      h.items[c] = static_cast<int>(items_.size());
+      items_.push_back({static_cast<int>(i), c, cls, n, cost});
+    }
+  }
+  // algorithmic work of one run (what the resident kernel executes per item)
+  for (auto& it : items_) {
+    const HostSolve& h = solves_[it.solve];
+    const int iters = std::max(1, h.in.iterations);
+    const bool refl = h.in.iterations > 0;
+    const double n = it.n, lg = std::log2(std::max(2.0, n));
+    double ffts = 1, passes = 0, pid_bytes = 0, src_bytes = 0;
+    for (int k = 0; k < iters; ++k) {
+      for (auto& st : h.steps) {
+        const int pf = st.fwd_t + (refl ? st.fwd_r : 0);
+        ffts += 1 + pf;
+        passes += pf;
+        if (st.pid >= 0) pid_bytes += n;
+        if (refl) src_bytes += 8.0 * st.niface + (k > 0 ? 12.0 * st.niface : 0.0);
+        if (!refl) continue;
+        ffts += 1 + st.bwd_t + st.bwd_r;
+        passes += st.bwd_t + st.bwd_r;
+        if (st.pid >= 0) pid_bytes += n;
+        src_bytes += 8.0 * st.niface + 12.0 * st.niface;
+      }
+      ffts += refl ? 2 : 0;
+    }
+    work_transforms_ += ffts;
+    work_flops_ += ffts * 5.0 * n * lg + passes * 6.0 * n;
+    work_bytes_ += pid_bytes + src_bytes + 3.0 * 8.0 * n;  // + input, transmitted, reflected
+  }
+  // order items by class, then by decreasing cost (longest first)
+  std::vector<int> order(items_.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    if (items_[a].cls != items_[b].cls) return items_[a].cls > items_[b].cls;
+    return items_[a].cost > items_[b].cost;
+  });
+  std::vector<Item> sorted;
+  for (int k : order) sorted.push_back(items_[k]);
+  items_ = sorted;
+  for (auto& h : solves_) h.items[0] = h.items[1] = -1;
+  for (std::size_t k = 0; k < items_.size(); ++k) solves_[items_[k].solve].items[items_[k].comp] = static_cast<int>(k);
+  for (int c = 0; c < kNumClasses; ++c) class_count_[c] = 0;
+  for (std::size_t k = 0; k < items_.size(); ++k) {
+    const int c = items_[k].cls;
+    if (class_count_[c] == 0) class_first_[c] = static_cast<int>(k);
+    ++class_count_[c];
+    class_maxn_[c] = std::max(class_maxn_[c], items_[k].n);
+  }
+  for (auto& it : items_) {
+    nlines += 3LL * it.n;  // input, transmitted, reflected
+    nsrc += 2 * solves_[it.solve].iface_count;
+    nweights += 2LL * it.n;
+    nenergy += 2LL * std::max(1, solves_[it.solve].in.iterations) + 1;
+  }
+  // allocate and upload pools
+  std::vector<R2Step> steps(nsteps);
+  std::vector<R2Pass> passes(npass);
+  std::vector<std::uint8_t> pids(npid);
+  std::vector<int> iface(niface);
+  std::vector<float> mask(nmask);
+  long long moff = 0;
+  std::vector<long long> mask_off(solves_.size(), -1);
+  for (std::size_t i = 0; i < solves_.size(); ++i) {
+    HostSolve& h = solves_[i];
+    std::copy(h.steps.begin(), h.steps.end(), steps.begin() + h.step_base);
+    std::copy(h.passes.begin(), h.passes.end(), passes.begin() + h.pass_base);
+    std::copy(h.pids.begin(), h.pids.end(), pids.begin() + h.pid_base);
+    std::copy(h.iface.begin(), h.iface.end(), iface.begin() + h.iface_base);
+    if (!h.in.mask.empty()) {  // hi values, then lo values (mask = hi + lo)
+      mask_off[i] = moff;
+      for (int q = 0; q < h.in.ny; ++q) {
+        const float hi = static_cast<float>(h.in.mask[q]);
+        mask[moff + q] = hi;
+        mask[moff + h.in.ny + q] = static_cast<float>(h.in.mask[q] - static_cast<double>(hi));
+      }
+      moff += 2LL * h.in.ny;
+    }
+  }
+  d_steps_.alloc(nsteps);
+  d_steps_.upload(steps.data(), nsteps);
+  d_passes_.alloc(std::max<long long>(npass, 1));
+  d_passes_.upload(passes.data(), npass);
+  d_pids_.alloc(std::max<long long>(npid, 1));
+  d_pids_.upload(pids.data(), npid);
+  d_iface_.alloc(std::max<long long>(niface, 1));
+  d_iface_.upload(iface.data(), niface);
+  d_mask_.alloc(std::max<long long>(nmask, 1));
+  d_mask_.upload(mask.data(), nmask);
+  d_tables_.alloc(std::max<long long>(ntab, 1));
+  d_twiddles_.alloc(tw.size());
+  d_twiddles_.upload(tw.data(), tw.size());
+  d_plans_.alloc(plans.size());
+  d_plans_.upload(plans.data(), plans.size());
+  d_lines_.alloc(nlines);
+  d_src_.alloc(std::max<long long>(nsrc, 1));
+  d_weights_.alloc(nweights);
+  d_energy_.alloc(nenergy);
+  d_clock_.alloc(2 * items_.size());
+  d_items_.alloc(items_.size());
+  d_queue_.alloc(kNumClasses);
+  d_io_.alloc(items_.size());
+  d_packed_in_.alloc(packed_total_);
+  d_packed_out_.alloc(2 * packed_total_);
+  check_cuda(cudaMemset(d_src_.ptr, 0, d_src_.bytes()), "memset");
+  check_cuda(cudaMemset(d_lines_.ptr, 0, d_lines_.bytes()), "memset");
+  // the uploads and memsets above run on the legacy default stream, which the non-blocking
+  // stream main_ does not wait for: finish them before any kernel on main_ touches the pools
+  check_cuda(cudaDeviceSynchronize(), "pool uploads");
+  // operator tables (FP64 on the device, stored as complex64)
+  std::vector<TableJob> tjobs;
+  for (auto& h : solves_)
+    for (std::size_t t = 0; t < h.tables.size(); ++t) {
+      const auto& [kind, nr, ns] = h.tables[t];
+      tjobs.push_back({d_tables_.ptr + h.table_base + static_cast<long long>(t) * 4 * h.in.ny, nr, ns,
+                       h.in.dy, h.in.k0, h.in.dz, h.in.ny, kind});
+    }
+  // item records, flux weights, packed-IO records
+  std::vector<WeightJob> wjobs;
+  std::vector<ItemIo> io(items_.size());
+  h_items_.resize(items_.size());
+  item_energy_off_.resize(items_.size());
+  long long loff = 0, soff = 0, woff = 0, eoff = 0;
+  for (std::size_t k = 0; k < items_.size(); ++k) {
+    const Item& itm = items_[k];
+    HostSolve& h = solves_[itm.solve];
+    const int n = h.in.ny;
+    R2Item r{};
+    r.input = d_lines_.ptr + loff;
+    r.transmitted = d_lines_.ptr + loff + n;
+    r.reflected = d_lines_.ptr + loff + 2 * n;
+    loff += 3LL * n;
+    r.tables = d_tables_.ptr + h.table_base + static_cast<long long>(itm.comp) * 2 * n;
+    r.src_fwd = d_src_.ptr + soff;
+    r.src_bwd = d_src_.ptr + soff + h.iface_count;
+    soff += 2 * h.iface_count;
+    r.mask = mask_off[itm.solve] >= 0 ? d_mask_.ptr + mask_off[itm.solve] : nullptr;
+    r.steps = d_steps_.ptr + h.step_base;
+    r.passes = d_passes_.ptr + h.pass_base;
+    r.pids = d_pids_.ptr + h.pid_base;
+    r.iface = d_iface_.ptr + h.iface_base;
+    r.w_out = d_weights_.ptr + woff;
+    r.w_in = d_weights_.ptr + woff + n;
+    // transmitted medium: label at the centre pixel of the last slab (src/bwpm/fast.py:148-151)
+    const cd last = h.in.indices[static_cast<std::size_t>(h.in.labels[static_cast<std::size_t>(h.in.nz - 1) * n + n / 2])];
+    wjobs.push_back({d_weights_.ptr + woff, last, h.in.dy, h.in.k0, n, itm.comp});
+    wjobs.push_back({d_weights_.ptr + woff + n, h.in.index_before, h.in.dy, h.in.k0, n, itm.comp});
+    woff += 2LL * n;
+    r.energy = d_energy_.ptr + eoff;
+    item_energy_off_[k] = eoff;
+    eoff += 2LL * std::max(1, h.in.iterations) + 1;
+    r.clock = d_clock_.ptr + 2 * k;
+    r.n = n;
+    r.nz = h.in.nz;
+    r.iterations = h.in.iterations;
+    r.plan = plan_of[n];
+    h_items_[k] = r;
+    io[k] = {h.packed, const_cast<cf*>(r.input), r.transmitted, r.reflected, n, itm.comp};
+  }
+  d_items_.upload(h_items_.data(), h_items_.size());
+  d_io_.upload(io.data(), io.size());
+  check_cuda(cudaDeviceSynchronize(), "item uploads");
+  if (!tjobs.empty()) {
+    DevBuf<TableJob> dj(tjobs.size());
+    dj.upload(tjobs.data(), tjobs.size());
+    check_cuda(cudaDeviceSynchronize(), "job upload");
+    int maxn = 0;
+    for (auto& j : tjobs) maxn = std::max(maxn, j.n);
+    for (std::size_t b = 0; b < tjobs.size(); b += 60000) {
+      const unsigned cnt = static_cast<unsigned>(std::min<std::size_t>(60000, tjobs.size() - b));
+      launch(k_table_jobs, dim3(ceil_div(maxn, 256), cnt), dim3(256), 0, main_, (const TableJob*)(dj.ptr + b));
+    }
+    check_cuda(cudaStreamSynchronize(main_), "tables");
+  }
+  {
+    DevBuf<WeightJob> dj(wjobs.size());
+    dj.upload(wjobs.data(), wjobs.size());
+    check_cuda(cudaDeviceSynchronize(), "job upload");
+    int maxn = 0;
+    for (auto& j : wjobs) maxn = std::max(maxn, j.n);
+    for (std::size_t b = 0; b < wjobs.size(); b += 60000) {
+      const unsigned cnt = static_cast<unsigned>(std::min<std::size_t>(60000, wjobs.size() - b));
+      launch(k_weight_jobs, dim3(ceil_div(maxn, 256), cnt), dim3(256), 0, main_, (const WeightJob*)(dj.ptr + b));
+    }
+    check_cuda(cudaStreamSynchronize(main_), "weights");
+  }
+  // inputs: packed complex128 of every solve -> per-item complex64 lines
+  std::vector<cd> packed(packed_total_);
+  for (auto& h : solves_) std::copy(h.in.field.begin(), h.in.field.end(), packed.begin() + h.packed);
+  d_packed_in_.upload(packed.data(), packed.size());
+  check_cuda(cudaDeviceSynchronize(), "input upload");
+  launch(k_unpack_inputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+         (const ItemIo*)d_io_.ptr, (const cd*)d_packed_in_.ptr);
+  check_cuda(cudaStreamSynchronize(main_), "inputs");
+  // launch shapes
+  auto set_attr = [](const void* k) {
+    check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024), "smem");
+  };
+  set_attr((const void*)k_resident2d<128>);
+  set_attr((const void*)k_resident2d<256>);
+  set_attr((const void*)k_resident2d<512>);
+  set_attr((const void*)k_resident2d<1024>);
+  for (int c = 0; c < kNumClasses; ++c) {
+    if (!class_count_[c]) continue;
+    const std::size_t smem = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+    int per_sm = 0;
+    const void* k = c == 0 ? (const void*)k_resident2d<128> : c == 1 ? (const void*)k_resident2d<256>
+                   : c == 2 ? (const void*)k_resident2d<512> : (const void*)k_resident2d<1024>;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kClassThreads[c], smem), "occupancy");
+    per_sm = std::max(1, per_sm);
+    class_grid_[c] = std::min(class_count_[c], per_sm * sms_);
+  }
+  bytes_ = d_steps_.bytes() + d_passes_.bytes() + d_pids_.bytes() + d_iface_.bytes() +
+           d_tables_.bytes() + d_twiddles_.bytes() + d_lines_.bytes() + d_src_.bytes() +
+           d_mask_.bytes() + d_weights_.bytes() + d_energy_.bytes() + d_packed_in_.bytes() +
+           d_packed_out_.bytes();
+  for (auto& h : solves_) {  // label planes live on the device now (pair ids, lists)
+    std::vector<std::int32_t>().swap(h.in.labels);
+    std::vector<std::uint8_t>().swap(h.pids);
+    std::vector<int>().swap(h.iface);
+    std::vector<R2Pass>().swap(h.passes);
+  }
+  prepared_ = true;
+}
+
+void Batch2DImpl::launch_classes(cudaStream_t origin) {
+  check_cuda(cudaMemsetAsync(d_queue_.ptr, 0, kNumClasses * sizeof(int), origin), "queue reset");
+  check_cuda(cudaEventRecord(ev0_, origin), "event");
+  // largest class first: its items are the longest chains
+  for (int c = kNumClasses - 1; c >= 0; --c) {
+    if (!class_count_[c]) continue;
+    cudaStream_t s = streams_[c];
+    check_cuda(cudaStreamWaitEvent(s, ev0_, 0), "wait");
+    const std::size_t smem = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+    const R2Item* items = d_items_.ptr + class_first_[c];
+    R2Shared sh{d_plans_.ptr, d_twiddles_.ptr};
+    const dim3 grid(class_grid_[c]);
+    int* q = d_queue_.ptr + c;
+    switch (c) {
+      case 0: launch(k_resident2d<128>, grid, dim3(128), smem, s, items, class_count_[c], q, sh); break;
+      case 1: launch(k_resident2d<256>, grid, dim3(256), smem, s, items, class_count_[c], q, sh); break;
+      case 2: launch(k_resident2d<512>, grid, dim3(512), smem, s, items, class_count_[c], q, sh); break;
+      default: launch(k_resident2d<1024>, grid, dim3(1024), smem, s, items, class_count_[c], q, sh);
+    }
+    check_cuda(cudaEventRecord(class_done_[c], s), "event");
+    check_cuda(cudaStreamWaitEvent(origin, class_done_[c], 0), "wait");
+  }
+}
+
+float Batch2DImpl::run() {
+  if (!prepared_) prepare();
+  check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+  cudaEvent_t start, stop;
+  check_cuda(cudaEventCreate(&start), "event");
+  check_cuda(cudaEventCreate(&stop), "event");
+  check_cuda(cudaEventRecord(start, main_), "event");
+  launch_classes(main_);
+  check_cuda(cudaEventRecord(stop, main_), "event");
+  check_cuda(cudaEventSynchronize(stop), "run");
+  float ms = 0;
+  check_cuda(cudaEventElapsedTime(&ms, start, stop), "elapsed");
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  return ms;
+}
+
+float Batch2DImpl::solve_packed(const cd* fields, cd* out) {
+  if (!prepared_) prepare();
+  check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+  cudaEvent_t start, stop;
+  check_cuda(cudaEventCreate(&start), "event");
+  check_cuda(cudaEventCreate(&stop), "event");
+  check_cuda(cudaEventRecord(start, main_), "event");
+  check_cuda(cudaMemcpyAsync(d_packed_in_.ptr, fields, packed_total_ * sizeof(cd), cudaMemcpyHostToDevice, main_), "h2d");
+  launch(k_unpack_inputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+         (const ItemIo*)d_io_.ptr, (const cd*)d_packed_in_.ptr);
+  launch_classes(main_);
+  check_cuda(cudaMemsetAsync(d_packed_out_.ptr, 0, d_packed_out_.bytes(), main_), "memset");
+  launch(k_pack_outputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+         (const ItemIo*)d_io_.ptr, d_packed_out_.ptr);
+  check_cuda(cudaMemcpyAsync(out, d_packed_out_.ptr, 2 * packed_total_ * sizeof(cd), cudaMemcpyDeviceToHost, main_), "d2h");
+  check_cuda(cudaEventRecord(stop, main_), "event");
+  check_cuda(cudaEventSynchronize(stop), "solve");
+  float ms = 0;
+  check_cuda(cudaEventElapsedTime(&ms, start, stop), "elapsed");
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  return ms;
+}
+
+void Batch2DImpl::result(std::int64_t id, Solve2DResult& r) {
+  if (!prepared_) throw invalid_argument("batch not run");
+  if (id < 0 || id >= static_cast<std::int64_t>(solves_.size())) throw invalid_argument("unknown solve id");
+  check_cuda(cudaStreamSynchronize(main_), "sync");
+  const HostSolve& h = solves_[id];
+  const int n = h.in.ny;
+  const int iters = std::max(1, h.in.iterations);
+  r.transmitted.assign(2 * n, cd{0.0, 0.0});
+  r.reflected.assign(2 * n, cd{0.0, 0.0});
+  r.flux_t.assign(h.in.iterations, 0.0);
+  r.flux_r.assign(h.in.iterations, 0.0);
+  r.flux_in = 0.0;
+  long long t0 = -1, t1 = -1;
+  std::vector<cf> line(n);
+  std::vector<double> en(2 * iters + 1);
+  for (int c = 0; c < 2; ++c) {
+    const int k = h.items[c];
+    if (k < 0) continue;
+    const R2Item& it = h_items_[k];
+    check_cuda(cudaMemcpy(line.data(), it.transmitted, n * sizeof(cf), cudaMemcpyDeviceToHost), "d2h");
+    for (int q = 0; q < n; ++q) r.transmitted[2 * q + c] = cast<double>(line[q]);
+    if (h.in.iterations > 0) {
+      check_cuda(cudaMemcpy(line.data(), it.reflected, n * sizeof(cf), cudaMemcpyDeviceToHost), "d2h");
+      for (int q = 0; q < n; ++q) r.reflected[2 * q + c] = cast<double>(line[q]);
+    }
+    check_cuda(cudaMemcpy(en.data(), it.energy, en.size() * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+    for (int i = 0; i < h.in.iterations; ++i) {
+      r.flux_t[i] += en[2 * i];
+      r.flux_r[i] += en[2 * i + 1];
+    }
+    r.flux_in += en[2 * iters];
+    long long clk[2];
+    check_cuda(cudaMemcpy(clk, it.clock, sizeof(clk), cudaMemcpyDeviceToHost), "d2h");
+    t0 = t0 < 0 ? clk[0] : std::min(t0, clk[0]);
+    t1 = std::max(t1, clk[1]);
+  }
+  r.latency_ms = t0 >= 0 ? static_cast<double>(t1 - t0) * 1e-6 : 0.0;
+}
+
+}  // namespace
+
+std::unique_ptr<Batch2D> make_batch2d(int device) { return std::make_unique<Batch2DImpl>(device); }
+
+}  // namespace bwpm

@@ -11,6 +11,7 @@
 
 #include "fft.cuh"
 #include "interface.cuh"
+#include "plane_kernels.cuh"
 
 namespace bwpm {
 
@@ -169,9 +170,9 @@ __global__ void k_dot_partial(const cx<T>* u, const cx<T>* v, long long m, cd* p
 
 // nx = 1: one CTA per component, the whole line in shared memory.
 template <int DIR, typename T>
-__global__ void k_line_fft(const cx<T>* in, cx<T>* out, int n, int ncomp, FftPlan plan,
-                           const cx<T>* __restrict__ tw) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPlaneThreads) k_line_fft(const cx<T>* in, cx<T>* out, int n, int ncomp, FftPlan plan,
+                           const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   for (int q = tid; q < n; q += nt) buf[q] = in[static_cast<long long>(q) * ncomp + c];
@@ -182,9 +183,9 @@ __global__ void k_line_fft(const cx<T>* in, cx<T>* out, int n, int ncomp, FftPla
 
 // y transform of `cols` columns × ncomp components per CTA; smem [y][col][comp].
 template <int DIR, typename T>
-__global__ void k_cols_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int cols,
-                           FftPlan plan, const cx<T>* __restrict__ tw) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPlaneThreads) k_cols_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int cols,
+                           FftPlan plan, const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int x0 = blockIdx.x * cols;
   const int tid = threadIdx.x, nt = blockDim.x;

@@ -5,10 +5,15 @@
 #include <string>
 
 #include "../../include/bwpm_b200.h"
+#include "batch2d.hpp"
 #include "solver.hpp"
 
 struct bwpm_solver {
   std::unique_ptr<bwpm::Solver> impl;
+};
+
+struct bwpm_batch {
+  std::unique_ptr<bwpm::Batch2D> impl;
 };
 
 namespace {
@@ -129,5 +134,129 @@ int bwpm_solver_stats(const bwpm_solver* s, int64_t* device_bytes, int64_t* kern
 }
 
 void bwpm_solver_destroy(bwpm_solver* s) { delete s; }
+
+int bwpm_batch_create(int device, bwpm_batch** out) {
+  return guarded([&] {
+    if (!out) throw bwpm::invalid_argument("null output handle");
+    auto b = std::make_unique<bwpm_batch>();
+    b->impl = bwpm::make_batch2d(device);
+    *out = b.release();
+  });
+}
+
+int bwpm_batch_add(bwpm_batch* b, size_t ny, double dy, double dz, double k0,
+                   const double* indices, size_t m, const int32_t* labels, size_t nz,
+                   double ib_re, double ib_im, const double* mask, const double* field,
+                   int iterations, int64_t* id) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
+    bwpm::Solve2D s;
+    s.ny = static_cast<int>(ny);
+    s.nz = static_cast<int>(nz);
+    s.dy = dy;
+    s.dz = dz;
+    s.k0 = k0;
+    s.indices.assign(as_cd(indices), as_cd(indices) + m);
+    s.labels.assign(labels, labels + nz * ny);
+    s.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) s.mask.assign(mask, mask + ny);
+    s.field.assign(as_cd(field), as_cd(field) + 2 * ny);
+    s.iterations = iterations;
+    const int64_t k = b->impl->add(std::move(s));
+    if (id) *id = k;
+  });
+}
+
+int bwpm_batch_prepare(bwpm_batch* b) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    b->impl->prepare();
+  });
+}
+
+int bwpm_batch_run(bwpm_batch* b, float* device_ms) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    const float ms = b->impl->run();
+    if (device_ms) *device_ms = ms;
+  });
+}
+
+int bwpm_batch_solve_packed(bwpm_batch* b, const double* fields, double* out, float* device_ms) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    if (!fields || !out) throw bwpm::invalid_argument("null array");
+    const float ms = b->impl->solve_packed(as_cd(fields), as_cd(out));
+    if (device_ms) *device_ms = ms;
+  });
+}
+
+int bwpm_batch_result(bwpm_batch* b, int64_t id, double* transmitted, double* reflected,
+                      double* flux_t, double* flux_r, double* flux_in, double* latency_ms) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    bwpm::Solve2DResult r;
+    b->impl->result(id, r);
+    if (transmitted) std::memcpy(transmitted, r.transmitted.data(), r.transmitted.size() * sizeof(bwpm::cd));
+    if (reflected) std::memcpy(reflected, r.reflected.data(), r.reflected.size() * sizeof(bwpm::cd));
+    if (flux_t) std::memcpy(flux_t, r.flux_t.data(), r.flux_t.size() * sizeof(double));
+    if (flux_r) std::memcpy(flux_r, r.flux_r.data(), r.flux_r.size() * sizeof(double));
+    if (flux_in) *flux_in = r.flux_in;
+    if (latency_ms) *latency_ms = r.latency_ms;
+  });
+}
+
+int bwpm_batch_stats(const bwpm_batch* b, int64_t* device_bytes, int64_t* kernel_launches,
+                     int64_t* work_items, int64_t* classes, int64_t* packed_inputs) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    if (device_bytes) *device_bytes = static_cast<int64_t>(b->impl->device_bytes());
+    if (kernel_launches) *kernel_launches = b->impl->kernel_launches();
+    if (work_items) *work_items = b->impl->work_items();
+    if (classes) *classes = b->impl->classes();
+    if (packed_inputs) *packed_inputs = static_cast<int64_t>(b->impl->packed_inputs());
+  });
+}
+
+int bwpm_batch_work(const bwpm_batch* b, double* transforms, double* flops, double* bytes) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    double t = 0, f = 0, y = 0;
+    b->impl->work(t, f, y);
+    if (transforms) *transforms = t;
+    if (flops) *flops = f;
+    if (bytes) *bytes = y;
+  });
+}
+
+void bwpm_batch_destroy(bwpm_batch* b) { delete b; }
+
+int bwpm_flush_l2(int device, size_t bytes) {
+  return guarded([&] {
+    static void* scratch[64] = {};
+    static size_t size[64] = {};
+    if (device < 0 || device >= 64) throw bwpm::invalid_argument("bad device");
+    bwpm::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    if (size[device] < bytes) {
+      if (scratch[device]) cudaFree(scratch[device]);
+      scratch[device] = nullptr;
+      bwpm::check_cuda(cudaMalloc(&scratch[device], bytes), "cudaMalloc");
+      size[device] = bytes;
+    }
+    bwpm::check_cuda(cudaMemset(scratch[device], size[device] & 0xff, bytes), "cudaMemset");
+    bwpm::check_cuda(cudaDeviceSynchronize(), "flush");
+  });
+}
+
+int bwpm_host_register(void* ptr, size_t bytes) {
+  return guarded([&] {
+    bwpm::check_cuda(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault), "cudaHostRegister");
+  });
+}
+
+int bwpm_host_unregister(void* ptr) {
+  return guarded([&] { bwpm::check_cuda(cudaHostUnregister(ptr), "cudaHostUnregister"); });
+}
 
 }  // extern "C"

@@ -88,16 +88,35 @@ inline HostPlan make_plan(int n) {
   return hp;
 }
 
-// Threads needed so that every stage fits its register staging (multiple of 32).
-inline int threads_needed(const FftPlan& p, int batch) {
+// Threads needed so that every stage fits its register staging of EPT values per thread
+// (multiple of 32).
+inline int threads_needed(const FftPlan& p, int batch, int ept = 16) {
   long long need = 32;
   for (int s = 0; s < p.nstages; ++s) {
     const int r = p.radix[s];
     const long long total = static_cast<long long>(p.n / r) * batch;
-    const long long t = (total + kmax_for(r) - 1) / kmax_for(r);
+    const long long k = kmax_for(r, ept);
+    const long long t = (total + k - 1) / k;
     need = std::max(need, t);
   }
   return static_cast<int>((need + 31) / 32 * 32);
+}
+
+// Twiddles in the kernel's storage: FP64 values, or FP32 (hi, lo) pairs rounded from FP64.
+template <typename T>
+inline std::vector<Tw<T>> twiddles_for(const HostPlan& hp) {
+  std::vector<Tw<T>> out(hp.twiddles.size());
+  for (std::size_t i = 0; i < out.size(); ++i) {
+    const cd w = hp.twiddles[i];
+    if constexpr (sizeof(T) == sizeof(double)) {
+      out[i].hi = cx<T>{static_cast<T>(w.re), static_cast<T>(w.im)};
+    } else {
+      const cf h{static_cast<float>(w.re), static_cast<float>(w.im)};
+      out[i].hi = h;
+      out[i].lo = cf{static_cast<float>(w.re - h.re), static_cast<float>(w.im - h.im)};
+    }
+  }
+  return out;
 }
 
 }  // namespace bwpm

@@ -21,6 +21,35 @@
 namespace bwpm {
 
 constexpr int kMaxPasses = 128;
+constexpr int kPlaneThreads = 512;  // CTA width limit of the plane kernels (128 registers)
+
+// Table entry times field value. FP64 tables hold one value per entry; FP32 tables hold the
+// FP64 value as hi + lo with the lo block `lo` entries after the hi block (see fft.cuh on why
+// constants recurring in every slab step are carried as pairs).
+template <typename T>
+__device__ __forceinline__ cx<T> tmul(cx<T> u, const cx<T>* m, long long q, long long lo) {
+  if constexpr (sizeof(T) == sizeof(double)) {
+    return u * m[q];
+  } else {
+    return pmul(u, m[q], m[lo + q]);
+  }
+}
+
+// Field value times the mask (FP32 masks hold hi values then lo values, `n` apart).
+template <typename T>
+__device__ __forceinline__ cx<T> mmul(cx<T> v, const T* mask, long long q, long long n) {
+  if constexpr (sizeof(T) == sizeof(double)) {
+    return v * mask[q];
+  } else {
+    return {fmaf(v.re, mask[q], v.re * mask[n + q]), fmaf(v.im, mask[q], v.im * mask[n + q])};
+  }
+}
+
+// Operator tables: 3 entries (m00, m01, m11) of N values; FP32 tables add the 3 lo blocks.
+template <typename T>
+constexpr int table_blocks() {
+  return sizeof(T) == sizeof(double) ? 3 : 6;
+}
 
 // Pass j of a step: pair index (into the step's pair-id plane), operator table, reflection flag.
 struct StepPasses {
@@ -47,8 +76,8 @@ struct Step2D {
 };
 
 template <typename T>
-__global__ void k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const cx<T>* __restrict__ tw) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPlaneThreads) k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int c = blockIdx.x;
   const int n = a.n, tid = threadIdx.x, nt = blockDim.x;
@@ -65,9 +94,9 @@ __global__ void k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const cx<T>* 
   for (int j = 0; j < ps.npass; ++j) {
     const cx<T>* m = static_cast<const cx<T>*>(ps.tab[j]) + e;
     if (keep_spec)
-      for (int q = tid; q < n; q += nt) buf[q] = spec[2 * q + c] * m[q];
+      for (int q = tid; q < n; q += nt) buf[q] = tmul(spec[2 * q + c], m, q, 3LL * n);
     else
-      for (int q = tid; q < n; q += nt) buf[q] = buf[q] * m[q];
+      for (int q = tid; q < n; q += nt) buf[q] = tmul(buf[q], m, q, 3LL * n);
     __syncthreads();
     fft_smem<+1>(buf, plan, tw, 1, tid, nt);
     const int pair = ps.pair[j];
@@ -75,7 +104,7 @@ __global__ void k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const cx<T>* 
       for (int q = tid; q < n; q += nt)
         if (!a.pid || a.pid[q] == pair) {
           cx<T> v = buf[q] * a.inv_n;
-          if (a.mask) v = v * a.mask[q];
+          if (a.mask) v = mmul(v, a.mask, q, n);
           a.out[2 * q + c] = v;
         }
     } else {
@@ -95,9 +124,9 @@ __global__ void k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const cx<T>* 
 
 // x transform of `rows` rows × ncomp interleaved components per CTA; smem [x][row][comp].
 template <int DIR, typename T>
-__global__ void k_rows_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int rows,
-                           FftPlan plan, const cx<T>* __restrict__ tw) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPlaneThreads) k_rows_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int rows,
+                           FftPlan plan, const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int y0 = blockIdx.x * rows;
   const int here = min(rows, ny - y0);
@@ -130,9 +159,9 @@ struct ColStep {
 // y transform of a tile of `cols` columns, then per pass: W = M·Ŝ (2×2), inverse y transform,
 // store to work plane j. smem: spectrum tile [y][col][2] and, for several passes, a work tile.
 template <typename T>
-__global__ void k_cols_step(ColStep<T> a, StepPasses ps, FftPlan plan,
-                            const cx<T>* __restrict__ tw) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, StepPasses ps, FftPlan plan,
+                            const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* sbuf = reinterpret_cast<cx<T>*>(smem_raw);
   const int ny = a.ny, nx = a.nx, cols = a.cols;
   const long long n = static_cast<long long>(ny) * nx;
@@ -165,10 +194,9 @@ __global__ void k_cols_step(ColStep<T> a, StepPasses ps, FftPlan plan,
         continue;
       }
       const long long q = static_cast<long long>(y) * nx + x;
-      const cx<T> m00 = m[q], m01 = m[n + q], m11 = m[2 * n + q];
       const cx<T> s0 = sbuf[2 * idx], s1 = sbuf[2 * idx + 1];
-      wbuf[2 * idx] = m00 * s0 + m01 * s1;
-      wbuf[2 * idx + 1] = m01 * s0 + m11 * s1;
+      wbuf[2 * idx] = tmul(s0, m, q, 3 * n) + tmul(s1, m + n, q, 3 * n);
+      wbuf[2 * idx + 1] = tmul(s0, m + n, q, 3 * n) + tmul(s1, m + 2 * n, q, 3 * n);
     }
     __syncthreads();
     fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
@@ -198,9 +226,9 @@ struct RowSelect {
 
 // inverse x transform of each pass for `rows` rows, then select/mask/gather/add.
 template <typename T>
-__global__ void k_rows_select(RowSelect<T> a, StepPasses ps, FftPlan plan,
-                              const cx<T>* __restrict__ tw) {
-  extern __shared__ unsigned char smem_raw[];
+__global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, StepPasses ps, FftPlan plan,
+                              const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int ny = a.ny, nx = a.nx, rows = a.rows;
   const long long n = static_cast<long long>(ny) * nx;
@@ -227,7 +255,7 @@ __global__ void k_rows_select(RowSelect<T> a, StepPasses ps, FftPlan plan,
         const long long q = static_cast<long long>(y0 + row) * nx + x;
         if (!a.pid || a.pid[q] == pair) {
           cx<T> v = buf[(x * rows + row) * 2 + c] * a.inv_n;
-          if (a.mask) v = v * a.mask[q];
+          if (a.mask) v = mmul(v, a.mask, q, n);
           a.out[2 * q + c] = v;
         }
       }
@@ -257,7 +285,7 @@ __global__ void k_add_plane(cx<T>* dst, const cx<T>* src, const T* mask, T scale
   // dst += src·scale (· mask per pixel when given); n2 = complex entries of an (N, 2) plane
   const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (i >= n2) return;
-  const cx<T> s = mask ? src[i] * (scale * mask[i >> 1]) : src[i] * scale;
+  const cx<T> s = mask ? mmul(src[i] * scale, mask, i >> 1, n2 >> 1) : src[i] * scale;
   dst[i] = dst[i] + s;
 }
 
@@ -277,9 +305,16 @@ __global__ void k_build_table(cx<T>* out, int kind, cd nr, cd ns, int ny, int nx
   const double ky = fftfreq(q / nx, ny, dy);
   cd m[3];
   operator_matrix(kind, kx, ky, nr, ns, k0, dz, m);
-  out[q] = cast<T>(m[0]);
-  out[n + q] = cast<T>(m[1]);
-  out[2 * n + q] = cast<T>(m[2]);
+  for (int e = 0; e < 3; ++e) {
+    if constexpr (sizeof(T) == sizeof(double)) {
+      out[e * n + q] = m[e];
+    } else {  // FP32 fields: M/N as hi + lo (the inverse transform's 1/N folded in)
+      const cd v = m[e] / static_cast<double>(n);
+      const cf hi = cast<float>(v);
+      out[e * n + q] = hi;
+      out[(3 + e) * n + q] = cf{static_cast<float>(v.re - hi.re), static_cast<float>(v.im - hi.im)};
+    }
+  }
 }
 
 }  // namespace bwpm

@@ -17,43 +17,13 @@
 #include <unordered_map>
 
 #include "born_kernels.cuh"
+#include "devbuf.hpp"
 #include "plan.hpp"
 #include "plane_kernels.cuh"
 #include "solver.hpp"
 
 namespace bwpm {
 namespace {
-
-template <typename U>
-struct DevBuf {
-  U* ptr = nullptr;
-  std::size_t n = 0;
-  DevBuf() = default;
-  explicit DevBuf(std::size_t count) { alloc(count); }
-  void alloc(std::size_t count) {
-    release();
-    n = count;
-    if (count) check_cuda(cudaMalloc(&ptr, count * sizeof(U)), "cudaMalloc");
-  }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    n = 0;
-  }
-  ~DevBuf() { release(); }
-  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), n(o.n) {
-    o.ptr = nullptr;
-    o.n = 0;
-  }
-  DevBuf& operator=(DevBuf&& o) noexcept {
-    std::swap(ptr, o.ptr);
-    std::swap(n, o.n);
-    return *this;
-  }
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  std::size_t bytes() const { return n * sizeof(U); }
-};
 
 constexpr int kThreads = 256;
 
@@ -122,7 +92,7 @@ class PlaneSolver final : public Solver {
   SolverInput in_;
   cudaStream_t stream_ = nullptr;
   HostPlan hy_, hx_;
-  DevBuf<C> tw_y_, tw_x_;
+  DevBuf<Tw<T>> tw_y_, tw_x_;
   std::vector<StepInfo> steps_;
   DevBuf<std::uint8_t> pid_pool_;
   DevBuf<int> iface_pool_, rowoff_pool_;
@@ -151,9 +121,9 @@ LaunchShape PlaneSolver<T>::rows_shape(int ncomp, int rows_max) const {
   LaunchShape s;
   const std::size_t row_bytes = in_.nx * ncomp * sizeof(C);
   s.rows = static_cast<int>(std::max<std::size_t>(1, std::min<std::size_t>(rows_max, 49152 / row_bytes)));
-  while (s.rows > 1 && threads_needed(hx_.plan, s.rows * ncomp) > 1024) --s.rows;
+  while (s.rows > 1 && threads_needed(hx_.plan, s.rows * ncomp) > kPlaneThreads) --s.rows;
   s.threads = std::max(64, threads_needed(hx_.plan, s.rows * ncomp));
-  if (s.threads > 1024) throw invalid_argument("nx too large for the row transform");
+  if (s.threads > kPlaneThreads) throw invalid_argument("nx too large for the row transform");
   s.smem = s.rows * row_bytes;
   return s;
 }
@@ -164,12 +134,12 @@ LaunchShape PlaneSolver<T>::cols_shape(int ncomp, int tiles) const {
   const std::size_t col_bytes = in_.ny * ncomp * sizeof(C);
   int cols = std::max(1, static_cast<int>(64 / (ncomp * sizeof(C))));
   while (cols > 1 && (col_bytes * cols * tiles > 98304 ||
-                      threads_needed(hy_.plan, cols * ncomp) > 1024))
+                      threads_needed(hy_.plan, cols * ncomp) > kPlaneThreads))
     --cols;
   s.rows = cols;
   s.threads = std::max(64, threads_needed(hy_.plan, cols * ncomp));
   s.smem = col_bytes * cols * tiles;
-  if (s.threads > 1024 || s.smem > 227 * 1024)
+  if (s.threads > kPlaneThreads || s.smem > 227 * 1024)
     throw invalid_argument("ny too large for the column transform");
   return s;
 }
@@ -211,11 +181,10 @@ void PlaneSolver<T>::setup() {
   check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   hy_ = make_plan(static_cast<int>(in_.ny));
   hx_ = make_plan(static_cast<int>(in_.nx));
-  auto upload_tw = [&](const HostPlan& hp, DevBuf<C>& d) {
-    std::vector<C> t(hp.twiddles.size());
-    for (std::size_t i = 0; i < t.size(); ++i) t[i] = cast<T>(hp.twiddles[i]);
+  auto upload_tw = [&](const HostPlan& hp, DevBuf<Tw<T>>& d) {
+    const std::vector<Tw<T>> t = twiddles_for<T>(hp);
     d.alloc(t.size());
-    check_cuda(cudaMemcpy(d.ptr, t.data(), t.size() * sizeof(C), cudaMemcpyHostToDevice), "twiddles");
+    d.upload(t.data(), t.size());
   };
   upload_tw(hy_, tw_y_);
   upload_tw(hx_, tw_x_);
@@ -296,10 +265,15 @@ void PlaneSolver<T>::setup() {
     check_cuda(cudaMemcpy(rowoff_pool_.ptr, rowoff_host.data(), rowoff_host.size() * sizeof(int),
                           cudaMemcpyHostToDevice), "rowoff");
   }
-  if (!in_.mask.empty()) {
-    std::vector<T> m(in_.mask.begin(), in_.mask.end());
-    mask_.alloc(nn);
-    check_cuda(cudaMemcpy(mask_.ptr, m.data(), nn * sizeof(T), cudaMemcpyHostToDevice), "mask");
+  if (!in_.mask.empty()) {  // FP32: hi values then lo values (mask = hi + lo)
+    const bool pair = sizeof(T) != sizeof(double);
+    std::vector<T> m((pair ? 2 : 1) * nn);
+    for (std::size_t q = 0; q < nn; ++q) {
+      m[q] = static_cast<T>(in_.mask[q]);
+      if (pair) m[nn + q] = static_cast<T>(in_.mask[q] - static_cast<double>(m[q]));
+    }
+    mask_.alloc(m.size());
+    mask_.upload(m.data(), m.size());
   }
   input_.alloc(2 * nn);
   e_.alloc(2 * nn);
@@ -309,7 +283,7 @@ void PlaneSolver<T>::setup() {
   // launch shapes and shared-memory opt-in
   if (is2d()) {
     thr2d_ = std::max(64, threads_needed(hy_.plan, 1));
-    if (thr2d_ > 1024 || nn * sizeof(C) > 227 * 1024)
+    if (thr2d_ > kPlaneThreads || nn * sizeof(C) > 227 * 1024)
       throw invalid_argument("ny too large for the single-CTA line transform");
     thr_line3_ = thr2d_;
     check_cuda(cudaFuncSetAttribute(k_step2d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
@@ -363,7 +337,7 @@ const cx<T>* PlaneSolver<T>::table(int kind, cd nr, cd ns) {
   auto key = std::make_tuple(kind, nr.re, nr.im, ns.re, ns.im);
   auto it = tables_.find(key);
   if (it != tables_.end()) return it->second.ptr;
-  DevBuf<C> t(3 * n());
+  DevBuf<C> t(table_blocks<T>() * n());
   launch(k_build_table<T>, dim3(ceil_div(n(), kThreads)), dim3(kThreads), 0, t.ptr, kind, nr, ns,
          static_cast<int>(in_.ny), static_cast<int>(in_.nx), in_.dy, in_.dx, in_.k0, in_.dz);
   const C* ptr = t.ptr;
@@ -403,7 +377,8 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   const StepPasses ps = passes(s, backward, reflect);
   const std::uint8_t* pid = st.pid_off >= 0 ? pid_pool_.ptr + st.pid_off : nullptr;
   const int* iface = st.niface > 0 ? iface_pool_.ptr + st.iface_off : nullptr;
-  const T inv_n = static_cast<T>(1.0 / static_cast<double>(n()));
+  // FP32 tables carry the inverse transform's 1/N already
+  const T inv_n = sizeof(T) == sizeof(double) ? static_cast<T>(1.0 / static_cast<double>(n())) : T(1);
   if (is2d()) {
     Step2D<T> a;
     a.in = in;

@@ -201,15 +201,27 @@ def microlens3d(n: int = 512, nz: int = 400, iterations: int = 6,
                    _vec(prof, "te"), iterations, name=f"microlens3d_{n}")
 
 
+def tilted_slab2d_params(rng: np.random.Generator, i: int, sizes=BATCH_SIZES,
+                         nz_range=(100, 2000), iterations: int = 6) -> dict:
+    """Parameters of one instance of the batched 2D workload (seeded by `rng`)."""
+    return {"i": i, "ny": int(rng.choice(sizes)),
+            "nz": int(rng.integers(nz_range[0], nz_range[1] + 1)),
+            "wl": float(rng.uniform(0.4, 1.0)), "theta": float(rng.uniform(0.0, np.deg2rad(30.0))),
+            "n": float(rng.uniform(1.4, 1.8)), "tilt": float(rng.uniform(0.0, np.deg2rad(8.0))),
+            "iterations": iterations}
+
+
 def tilted_slab2d(rng: np.random.Generator, i: int, sizes=BATCH_SIZES,
                   nz_range=(100, 2000), iterations: int = 6) -> Problem:
     """One instance of the batched 2D workload (seeded by `rng`)."""
-    ny = int(rng.choice(sizes))
-    nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
-    wl = float(rng.uniform(0.4, 1.0))
-    theta = float(rng.uniform(0.0, np.deg2rad(30.0)))
-    n = float(rng.uniform(1.4, 1.8))
-    tilt = float(rng.uniform(0.0, np.deg2rad(8.0)))
+    return tilted_slab2d_from(tilted_slab2d_params(rng, i, sizes, nz_range, iterations))
+
+
+def tilted_slab2d_from(prm: dict) -> Problem:
+    """Builds the instance: one slab n in air, front face tilted, back face flat (middle half
+    of nz), tilted Gaussian beam w₀ = ny·dy/8, mask width ny·dy/10 (order 8), TE for even i."""
+    i, ny, nz, wl = prm["i"], prm["ny"], prm["nz"], prm["wl"]
+    theta, n, tilt, iterations = prm["theta"], prm["n"], prm["tilt"], prm["iterations"]
     lam = wl * 1e-3
     dy, dz = lam / 8, lam / 10
     k0 = k0_of(wl)
@@ -228,11 +240,17 @@ def tilted_slab2d(rng: np.random.Generator, i: int, sizes=BATCH_SIZES,
                    extra={"wavelength_um": wl, "theta": theta, "tilt": tilt})
 
 
+def batch2d_params(count: int = 256, seed: int = 4, sizes=BATCH_SIZES, nz_range=(100, 2000),
+                   iterations: int = 6) -> list[dict]:
+    """Parameters of the batched 2D workload (cheap; build each with tilted_slab2d_from)."""
+    rng = np.random.default_rng(seed)
+    return [tilted_slab2d_params(rng, i, sizes, nz_range, iterations) for i in range(count)]
+
+
 def batch2d(count: int = 256, seed: int = 4, sizes=BATCH_SIZES, nz_range=(100, 2000),
             iterations: int = 6) -> list[Problem]:
     """The batched 2D workload: `count` seeded instances of uneven size."""
-    rng = np.random.default_rng(seed)
-    return [tilted_slab2d(rng, i, sizes, nz_range, iterations) for i in range(count)]
+    return [tilted_slab2d_from(p) for p in batch2d_params(count, seed, sizes, nz_range, iterations)]
 
 
 def smooth_sizes(lo: int, hi: int) -> list[int]:

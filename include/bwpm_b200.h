@@ -77,6 +77,55 @@ int bwpm_solver_stats(const bwpm_solver* s, int64_t* device_bytes, int64_t* kern
 /* Releases the solver (CudaSolver destructor, cpp/src/solver_cuda.cu:721-727). */
 void bwpm_solver_destroy(bwpm_solver* s);
 
+/* ---- batched 2D solves (complex64 fields; no counterpart in the reference, which solves one
+ * problem per CudaSolver.run call: cpp/src/solver_cuda.cu:729). Each solve is a 2D problem in the
+ * reference's 2D convention (src/bwpm/fast.py:120-142: nx = 1, lateral axis y). All solves of a
+ * batch run in one launch of persistent kernels; see bwpm_b200/csrc/resident2d.cuh. */
+typedef struct bwpm_batch bwpm_batch;
+
+int bwpm_batch_create(int device, bwpm_batch** out);
+
+/* Adds one solve: labels nz·ny int32, mask ny doubles or NULL, field ny·2 complex; *id gets its
+ * index. Same validation and messages as bwpm_solver_create. */
+int bwpm_batch_add(bwpm_batch* b, size_t ny, double dy, double dz, double k0,
+                   const double* indices, size_t m, const int32_t* labels, size_t nz,
+                   double index_before_re, double index_before_im, const double* mask,
+                   const double* field, int iterations, int64_t* id);
+
+/* Builds the device pools, operator tables and launch shapes (once, after the last add). */
+int bwpm_batch_prepare(bwpm_batch* b);
+
+/* Solves every added problem once with the inputs already on the device; device_ms gets the
+ * CUDA-event time of the launch. */
+int bwpm_batch_run(bwpm_batch* b, float* device_ms);
+
+/* End to end: copies new incident fields (packed: Σ ny·2 complex in add order) to the device,
+ * solves, and copies (transmitted ny·2, reflected ny·2) per solve back into out (packed);
+ * device_ms covers copies and kernels. */
+int bwpm_batch_solve_packed(bwpm_batch* b, const double* fields, double* out, float* device_ms);
+
+/* Results of solve `id` after a run: transmitted/reflected ny·2 complex; flux_t/flux_r
+ * (iterations values, power flux per iteration as src/bwpm/fpwpm.py:205-216); flux_in; device
+ * latency of the solve in ms. Any pointer may be NULL. */
+int bwpm_batch_result(bwpm_batch* b, int64_t id, double* transmitted, double* reflected,
+                      double* flux_t, double* flux_r, double* flux_in, double* latency_ms);
+
+int bwpm_batch_stats(const bwpm_batch* b, int64_t* device_bytes, int64_t* kernel_launches,
+                     int64_t* work_items, int64_t* classes, int64_t* packed_inputs);
+
+/* Algorithmic work of one run: transforms, FLOPs (5·N·log2 N per transform, 6·N per spectral
+ * multiply) and minimal DRAM bytes (pair ids, sparse sources, incident and output fields). */
+int bwpm_batch_work(const bwpm_batch* b, double* transforms, double* flops, double* bytes);
+
+void bwpm_batch_destroy(bwpm_batch* b);
+
+/* Writes `bytes` of scratch memory on `device` (evicts the 126 MB L2 between timed runs). */
+int bwpm_flush_l2(int device, size_t bytes);
+
+/* Page-locks host memory for fast copies (cudaHostRegister) and releases it. */
+int bwpm_host_register(void* ptr, size_t bytes);
+int bwpm_host_unregister(void* ptr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,152 @@
+"""Batched resident 2D engine (complex64) against the FP64 references, on a GPU.
+
+Tolerances: relative L2 ≤ 1e-4 on transmitted/reflected fields against FP64 (the reference's
+golden files, the reference CPU core outputs, or the FP64 GPU path that matches them at 1e-10),
+and |ε_c64 − ε_FP64| ≤ 1e-6·max(1, (P_R + P_T)/P_in) on the energy residual
+ε = 1 − (P_R + P_T)/P_in (the balance relative to the largest of the fluxes involved).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, load_npz, rel_l2
+from golden_cases import case_2d
+
+pytestmark = pytest.mark.gpu
+
+L2_C64 = 1e-4
+EPS_TOL = 1e-6
+
+
+def _add_case(b, name, iters):
+    args, f, fl, a, meta = case_2d(name)
+    ny, _, dy, _, dz, k0, indices, labels, ib, mask = args
+    i = b.add(ny, dy, dz, k0, indices, labels, ib, None if mask is None else mask[:, 0],
+              f[:, 0, :], iters)
+    return i, a
+
+
+def test_batch_golden_2d_cases():
+    from bwpm_b200.batch import Batch2D
+
+    b = Batch2D()
+    i1, a1 = _add_case(b, "fpwpm2d_interface", 0)
+    i2, a2 = _add_case(b, "bwpm2d_tilted_silver", 2)
+    i3, a3 = _add_case(b, "bwpm2d_slab_exact", 40)
+    b.prepare()
+    b.run()
+    r1, r2, r3 = b.result(i1), b.result(i2), b.result(i3)
+    assert rel_l2(r1["transmitted"], a1["expected.planes"][-1]) < L2_C64
+    assert rel_l2(r2["transmitted"], a2["expected.forward"][-1]) < L2_C64
+    assert rel_l2(r2["reflected"], a2["expected.backward"][0]) < L2_C64
+    assert np.max(np.abs(np.array(r2["energy_residual"]) - a2["expected.energy_residual"])) < EPS_TOL
+    assert rel_l2(r3["transmitted"], a3["expected.transmitted"]) < L2_C64
+    assert rel_l2(r3["reflected"], a3["expected.reflected"]) < L2_C64
+    assert np.all(r1["reflected"] == 0)
+
+
+@pytest.mark.parametrize("name", ["slab2d_te", "slab2d_tm"])
+def test_batch_slab_full_size(name):
+    """1024 points, 250 slabs, 8 iterations against the reference CPU core (FP64)."""
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import Batch2D
+
+    d = load_npz("workload_cases.npz")
+    prob = workloads.Problem.from_arrays(d, name + ".")
+    b = Batch2D()
+    i = b.add_problem(prob)
+    b.run()
+    r = b.result(i)
+    assert rel_l2(r["transmitted"], d[name + ".transmitted"][:, 0]) < L2_C64
+    assert rel_l2(r["reflected"], d[name + ".reflected"][:, 0]) < L2_C64
+
+
+def _fp64(prob):
+    from bwpm_b200 import _core
+
+    s = _core.CudaSolver(*prob.core_args(), 0)
+    return s.run(prob.field, prob.iterations, [])
+
+
+def test_batch_uneven_instances_against_fp64_and_energy():
+    """Uneven sizes incl. 3·2^k, tilted faces, masks, TE and TM, 0-30° incidence."""
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import Batch2D
+    from bwpm_b200.model import Grid2D, power_flux
+
+    probs = workloads.batch2d(count=12, seed=11, sizes=(256, 384, 768, 1536, 3072, 6144),
+                              nz_range=(40, 120), iterations=3)
+    b = Batch2D()
+    ids = [b.add_problem(p) for p in probs]
+    b.run()
+    for p, i in zip(probs, ids):
+        r = b.result(i)
+        ref = _fp64(p)
+        assert rel_l2(r["transmitted"], ref["transmitted"][:, 0]) < L2_C64, p.name
+        assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64, p.name
+        g = Grid2D(p.ny, p.dy, p.dz, p.extra["wavelength_um"])
+        p_in = power_flux(p.field[:, 0], g, p.index_before)
+        last = complex(p.indices[int(p.labels[-1, p.ny // 2, 0])])
+        for k in range(p.iterations):
+            pt = power_flux(ref["transmitted_iter"][k][:, 0], g, last)
+            pr = power_flux(ref["reflected_iter"][k][:, 0], g, p.index_before, direction=-1)
+            eps64 = 1.0 - (pt + pr) / p_in
+            scale = max(1.0, (pt + pr) / p_in)
+            assert abs(r["energy_residual"][k] - eps64) < EPS_TOL * scale, (p.name, k)
+
+
+def test_two_classes_in_one_batch():
+    """A 6144-point and a 256-point solve (two CTA-width classes run concurrently)."""
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import Batch2D
+
+    probs = workloads.batch2d(count=12, seed=11, sizes=(256, 384, 768, 1536, 3072, 6144),
+                              nz_range=(40, 120), iterations=3)
+    b = Batch2D()
+    ids = [b.add_problem(probs[2]), b.add_problem(probs[0])]
+    b.run()
+    for p, i in zip((probs[2], probs[0]), ids):
+        ref = _fp64(p)
+        assert rel_l2(b.result(i)["transmitted"], ref["transmitted"][:, 0]) < L2_C64
+
+
+def test_result_alone_equals_result_in_mix():
+    """A solve run alone and inside a batch of other solves gives the same result."""
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import Batch2D
+
+    probs = workloads.batch2d(count=9, seed=12, sizes=(256, 512, 1024, 3072),
+                              nz_range=(30, 80), iterations=2)
+    alone = Batch2D()
+    ia = alone.add_problem(probs[0])
+    alone.run()
+    ra = alone.result(ia)
+    mix = Batch2D()
+    ids = [mix.add_problem(p) for p in probs[1:5]] + [mix.add_problem(probs[0])] + [
+        mix.add_problem(p) for p in probs[5:]]
+    mix.run()
+    rm = mix.result(ids[4])
+    assert np.array_equal(ra["transmitted"], rm["transmitted"])
+    assert np.array_equal(ra["reflected"], rm["reflected"])
+
+
+def test_solve_packed_round_trip():
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import Batch2D
+
+    probs = workloads.batch2d(count=5, seed=13, sizes=(256, 1024), nz_range=(20, 40), iterations=2)
+    b = Batch2D()
+    ids = [b.add_problem(p) for p in probs]
+    b.run()
+    fields = np.concatenate([p.field[:, 0, :].ravel() for p in probs])
+    out = np.empty(2 * fields.size, dtype=np.complex128)
+    b.solve_packed(fields, out)
+    off = 0
+    for p, i in zip(probs, ids):
+        r = b.result(i)
+        n2 = 2 * p.ny
+        assert np.array_equal(out[off:off + n2].reshape(p.ny, 2), r["transmitted"])
+        assert np.array_equal(out[off + n2:off + 2 * n2].reshape(p.ny, 2), r["reflected"])
+        off += 2 * n2
