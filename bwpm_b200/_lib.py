@@ -51,6 +51,7 @@ SIGNATURES: dict[str, tuple] = {
     "bwpm_batch_work": (_i, [_p, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d)]),
     "bwpm_batch_destroy": (None, [_p]),
     "bwpm_flush_l2": (_i, [_i, _sz]),
+    "bwpm_step2d_noalloc": (_i, [_i, _sz, _d, _d, _d, _p, _sz, _p, _p, _d, _d, _p, _p, _p, _p]),
     "bwpm_host_register": (_i, [_p, _sz]),
     "bwpm_host_unregister": (_i, [_p]),
 }

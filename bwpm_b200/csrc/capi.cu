@@ -6,6 +6,7 @@
 
 #include "../../include/bwpm_b200.h"
 #include "batch2d.hpp"
+#include "noalloc.hpp"
 #include "solver.hpp"
 
 struct bwpm_solver {
@@ -246,6 +247,21 @@ int bwpm_flush_l2(int device, size_t bytes) {
     }
     bwpm::check_cuda(cudaMemset(scratch[device], size[device] & 0xff, bytes), "cudaMemset");
     bwpm::check_cuda(cudaDeviceSynchronize(), "flush");
+  });
+}
+
+static_assert(BWPM_NOALLOC_MAX_N == bwpm::kNoAllocMaxN, "header and library disagree");
+static_assert(BWPM_NOALLOC_SCRATCH_BYTES == bwpm::kNoAllocScratchBytes, "header and library disagree");
+
+int bwpm_step2d_noalloc(int device, size_t ny, double dy, double dz, double k0,
+                        const double* indices, size_t m, const int32_t* labels_before,
+                        const int32_t* labels_after, double ib_re, double ib_im,
+                        const double* mask, const double* field_in, double* field_out,
+                        void* stream) {
+  return guarded([&] {
+    bwpm::step2d_noalloc(device, ny, dy, dz, k0, as_cd(indices), m, labels_before, labels_after,
+                         bwpm::cd{ib_re, ib_im}, mask, as_cd(field_in), as_cd(field_out),
+                         static_cast<cudaStream_t>(stream));
   });
 }
 

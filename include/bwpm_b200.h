@@ -122,6 +122,31 @@ void bwpm_batch_destroy(bwpm_batch* b);
 /* Writes `bytes` of scratch memory on `device` (evicts the 126 MB L2 between timed runs). */
 int bwpm_flush_l2(int device, size_t bytes);
 
+/* ---- allocation-free slab step (no counterpart in the reference) ----------------------------
+ * One FP64 forward transmission step of a 2D field (the reference's 2D convention: nx = 1,
+ * lateral axis y), the same operation as one slab of bwpm_solver_run with iterations = 0:
+ * out = mask · Σ_(r,s) I_r,s F⁻¹{T_r,s e^{i k_z,s dz} F{in}}. For callers that cannot allocate
+ * device memory when they need the step (a host framework that owns all device memory through
+ * its own arena, a real-time loop that must not allocate after start-up, a plugin with a fixed
+ * memory budget): it calls no cudaMalloc or cudaFree. Its scratch (the spectrum of `field_in`
+ * and the FFT twiddles) is one fixed device array of BWPM_NOALLOC_SCRATCH_BYTES bytes that every
+ * GPU loading this library holds until exit; the array keeps the last call's contents and all
+ * calls on a device share it, so calls that overlap on the GPU (other threads or streams) race.
+ * The first call on a device looks up the array's address; make that first call before any
+ * stream capture. The call waits for its stream before returning.
+ * Device pointers: field_in/field_out ny·2 complex, labels_before/labels_after ny int32
+ * (labels_before NULL: the medium before the volume, index_before), mask ny doubles or NULL.
+ * indices: host array of m ≤ 32 complex. Limits: 2 ≤ ny ≤ BWPM_NOALLOC_MAX_N, ny a product of
+ * 2, 3, 5 and 7; anything else returns BWPM_EINVAL with a message. stream: a cudaStream_t or
+ * NULL for the default stream. */
+#define BWPM_NOALLOC_MAX_N 8192
+#define BWPM_NOALLOC_SCRATCH_BYTES 393472
+int bwpm_step2d_noalloc(int device, size_t ny, double dy, double dz, double k0,
+                        const double* indices, size_t m, const int32_t* labels_before,
+                        const int32_t* labels_after, double index_before_re,
+                        double index_before_im, const double* mask, const double* field_in,
+                        double* field_out, void* stream);
+
 /* Page-locks host memory for fast copies (cudaHostRegister) and releases it. */
 int bwpm_host_register(void* ptr, size_t bytes);
 int bwpm_host_unregister(void* ptr);
