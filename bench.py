@@ -37,6 +37,7 @@ WORKLOAD = ("batched-2d: 256 seeded tilted-slab solves, ny 256-8192 incl. 3*2^k,
             "lambda 0.4-1.0 um, 0-30 deg incidence, n 1.4-1.8, 0-8 deg tilt, mask, TE/TM, "
             "6 iterations")
 COUNT, SEED = 256, 4
+REDUCED: dict = {}  # set by --reduced (profiling runs); empty for the benchmark itself
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs × FP32 lanes × FMA × max clock
 
 
@@ -210,7 +211,11 @@ def _dist_for_reference():
 def _params():
     from bwpm_b200 import workloads
 
-    return workloads.batch2d_params(COUNT, SEED)
+    prm = workloads.batch2d_params(COUNT, SEED)
+    if REDUCED:  # reduced case for profiling: fewer solves, shorter chains
+        prm = [dict(p, nz=min(p["nz"], REDUCED["nz_max"]), iterations=REDUCED["iterations"])
+               for p in prm[: REDUCED["count"]]]
+    return prm
 
 
 # ---- our arm ----------------------------------------------------------------------------------
@@ -250,7 +255,8 @@ def run_ours(args) -> None:
             times.append(b.run())
     clocks = clk.summary()
     step_ms = _max_over_ranks(dist, float(np.sum(times))) / args.steps
-    lat = np.array([b.result(i)["latency_ms"] for i in range(COUNT)])
+    count = len(params)
+    lat = np.array([b.result(i)["latency_ms"] for i in range(count)])
     # end to end through the public API: H2D of incident fields, solve, D2H of results
     e2e_times = []
     for _ in range(max(1, args.warmup // 2)):
@@ -264,11 +270,11 @@ def run_ours(args) -> None:
     if rank != 0:
         _barrier(dist)
         return
-    value = ws * COUNT / (step_ms * 1e-3)
+    value = ws * count / (step_ms * 1e-3)
     # plain per-solve FP64 GPU path (drop-in CudaSolver) on a seeded sample; L2 error of the
     # batched complex64 results against it
     rng = np.random.default_rng(7)
-    sample = [int(i) for i in rng.permutation(COUNT)[: args.fp64_sample]]
+    sample = [int(i) for i in rng.permutation(count)[: args.fp64_sample]]
     fp64_t, errs, eps_err = [], [], []
     for i in sample:
         p = workloads.tilted_slab2d_from(params[i])
@@ -291,8 +297,8 @@ def run_ours(args) -> None:
                            / max(1.0, (pt + pr) / p_in))
         del s
     mean_cost = np.mean([prm["ny"] * np.log2(prm["ny"]) * prm["nz"] for prm in params])
-    samp_cost = np.mean([params[i]["ny"] * np.log2(params[i]["ny"]) * params[i]["nz"] for i in sample])
-    fp64_rate = 1.0 / (np.mean(fp64_t) * mean_cost / samp_cost)
+    samp_cost = np.mean([params[i]["ny"] * np.log2(params[i]["ny"]) * params[i]["nz"] for i in sample]) if sample else 1.0
+    fp64_rate = 1.0 / (np.mean(fp64_t) * mean_cost / samp_cost) if sample else None
     # roofline of the resident kernel: algorithmic FLOPs per launch ÷ launch time
     kern_s = step_ms * 1e-3
     achieved = work["flops"] / kern_s / 1e12
@@ -302,18 +308,19 @@ def run_ours(args) -> None:
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "global_batch": COUNT * ws, "seq_len": None,
+        "config": {"workload": WORKLOAD if not REDUCED else f"REDUCED profiling case {REDUCED}",
+                   "global_batch": count * ws, "seq_len": None,
                    "parallelism": f"replicas{ws}", "l2": "flushed (512 MB write) before each timed step",
                    "work_items": stats["work_items"], "classes": stats["classes"]},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "fp64_plain": {"value": fp64_rate, "unit": "solves/s", "sample": len(sample),
                        "note": "per-solve FP64 CudaSolver (drop-in path), mean sample time scaled "
                                "to the batch's mean N·log2N·nz",
-                       "speedup_batched_c64": value / ws / fp64_rate},
-        "l2_err_max": float(np.max(errs)),
+                       "speedup_batched_c64": value / ws / fp64_rate if fp64_rate else None},
+        "l2_err_max": float(np.max(errs)) if errs else None,
         "eps_err_max": float(np.max(eps_err)) if eps_err else None,
         "eps_err_note": "|eps_c64 - eps_fp64| / max(1, (P_R + P_T)/P_in) over the sample's iterations",
-        "e2e": {"value": ws * COUNT / (e2e_ms * 1e-3), "unit": "solves/s",
+        "e2e": {"value": ws * count / (e2e_ms * 1e-3), "unit": "solves/s",
                 "h2d_bytes_per_step": int(packed_in.nbytes), "d2h_bytes_per_step": int(packed_out.nbytes)},
         "gpu_launches": int(stats["classes"]) * args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS,
@@ -353,7 +360,15 @@ def main() -> None:
     ap.add_argument("--fp64-sample", type=int, default=6)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="target CPU seconds per core")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--reduced", type=str, default="",
+                    help="profiling only: COUNT,NZ_MAX,ITERATIONS (first COUNT solves, chains "
+                         "capped); skips the FP64 and CPU comparisons")
     args = ap.parse_args()
+    if args.reduced:
+        c, z, it = (int(v) for v in args.reduced.split(","))
+        REDUCED.update(count=c, nz_max=z, iterations=it)
+        args.no_cpu = True
+        args.fp64_sample = 0
     if args.impl == "reference":
         run_reference(args)
     else:

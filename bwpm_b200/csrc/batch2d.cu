@@ -26,8 +26,41 @@
 namespace bwpm {
 namespace {
 
-constexpr int kClassThreads[] = {128, 256, 512, 1024};
-constexpr int kNumClasses = 4;
+constexpr int kClassThreads[] = {64, 128, 256, 512};
+constexpr int kGenericClasses = 4;
+
+// Lengths with a compile-time register-resident kernel: N, threads, radices (each divides N/NT).
+struct FixedSpec {
+  int n, nt;
+  std::vector<int> radices;
+};
+const std::vector<FixedSpec>& fixed_specs() {
+  static const std::vector<FixedSpec> specs = {
+      {256, 32, {8, 8, 4}},         {384, 32, {4, 4, 4, 3, 2}},  {512, 32, {16, 8, 4}},
+      {768, 64, {4, 4, 4, 4, 3}},   {1024, 64, {16, 16, 4}},     {1536, 64, {8, 8, 8, 3}},
+      {2048, 128, {16, 16, 8}},     {3072, 128, {8, 8, 8, 3, 2}}, {4096, 256, {16, 16, 16}},
+      {6144, 256, {8, 8, 8, 4, 3}}, {8192, 512, {8, 8, 8, 8, 2}}};
+  return specs;
+}
+constexpr int kNumClasses = kGenericClasses + 11;  // class index ≥ kGenericClasses: fixed spec
+
+using rf::Radices;
+// kernel entry of the fixed spec with index `i` (same order as fixed_specs())
+const void* fixed_kernel(int i) {
+  switch (i) {
+    case 0: return (const void*)k_resident2d_fixed<256, 32, Radices<8, 8, 4>>;
+    case 1: return (const void*)k_resident2d_fixed<384, 32, Radices<4, 4, 4, 3, 2>>;
+    case 2: return (const void*)k_resident2d_fixed<512, 32, Radices<16, 8, 4>>;
+    case 3: return (const void*)k_resident2d_fixed<768, 64, Radices<4, 4, 4, 4, 3>>;
+    case 4: return (const void*)k_resident2d_fixed<1024, 64, Radices<16, 16, 4>>;
+    case 5: return (const void*)k_resident2d_fixed<1536, 64, Radices<8, 8, 8, 3>>;
+    case 6: return (const void*)k_resident2d_fixed<2048, 128, Radices<16, 16, 8>>;
+    case 7: return (const void*)k_resident2d_fixed<3072, 128, Radices<8, 8, 8, 3, 2>>;
+    case 8: return (const void*)k_resident2d_fixed<4096, 256, Radices<16, 16, 16>>;
+    case 9: return (const void*)k_resident2d_fixed<6144, 256, Radices<8, 8, 8, 4, 3>>;
+    default: return (const void*)k_resident2d_fixed<8192, 512, Radices<8, 8, 8, 8, 2>>;
+  }
+}
 
 // Operator table job: M/N of `kind` for (ñ_r, ñ_s), entry m00 (E_x) at out[0..2N) and m11 (E_y)
 // at out[2N..4N), each as N hi values then N lo values with M/N = hi + lo (built in FP64; the
@@ -205,6 +238,11 @@ class Batch2DImpl final : public Batch2D {
   int class_first_[kNumClasses] = {};
   int class_maxn_[kNumClasses] = {};
   int class_grid_[kNumClasses] = {};
+  int class_threads_[kNumClasses] = {};
+  std::size_t class_smem_[kNumClasses] = {};
+  const void* class_fn_[kNumClasses] = {};
+  std::map<int, int> plan_twbase_, plan_fixed_;
+  bool fixed_enabled_ = true;
   // device pools
   DevBuf<R2Step> d_steps_;
   DevBuf<R2Pass> d_passes_;
@@ -350,8 +388,13 @@ void Batch2DImpl::prepare() {
   for (auto& h : solves_) {
     const int n = h.in.ny;
     if (plan_of.count(n)) continue;
-    HostPlan hp = make_plan(n);
+    int fixed = -1;
+    for (std::size_t f = 0; f < fixed_specs().size(); ++f)
+      if (fixed_specs()[f].n == n && fixed_enabled_) fixed = static_cast<int>(f);
+    HostPlan hp = fixed >= 0 ? make_plan_radices(n, fixed_specs()[fixed].radices) : make_plan(n);
     const int base = static_cast<int>(tw.size());
+    plan_twbase_[n] = base;
+    plan_fixed_[n] = fixed;
     for (auto& t : twiddles_for<float>(hp)) tw.push_back(t);
     for (int s = 0; s < hp.plan.nstages; ++s) hp.plan.twoff[s] += base;
     hp.plan.rootoff += base;
@@ -385,10 +428,14 @@ void Batch2DImpl::prepare() {
       for (int q = 0; q < n && !any; ++q) any = h.in.field[2 * q + c].re != 0.0 || h.in.field[2 * q + c].im != 0.0;
       if (!any) continue;
       int cls = 0;
-      const int want = threads_needed(plans[plan_of[n]], 1, kR2Ept);
-      if (want > kClassThreads[kNumClasses - 1])
-        throw invalid_argument("ny = " + std::to_string(n) + " needs more than 1024 threads in the resident 2D engine");
-      while (cls < kNumClasses - 1 && kClassThreads[cls] < want) ++cls;
+      if (plan_fixed_[n] >= 0) {
+        cls = kGenericClasses + plan_fixed_[n];
+      } else {
+        const int want = threads_needed(plans[plan_of[n]], 1, kR2Ept);
+        if (want > kClassThreads[kGenericClasses - 1])
+          throw invalid_argument("ny = " + std::to_string(n) + " needs more than 512 threads in the resident 2D engine");
+        while (cls < kGenericClasses - 1 && kClassThreads[cls] < want) ++cls;
+      }
       double passes = 0;
       for (auto& st : h.steps) passes += 2 + st.fwd_t + st.fwd_r + st.bwd_t + st.bwd_r;
       const double cost = std::max(1, h.in.iterations) * passes * n * std::log2(std::max(2, n));
@@ -590,19 +637,32 @@ void Batch2DImpl::prepare() {
   auto set_attr = [](const void* k) {
     check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024), "smem");
   };
+  set_attr((const void*)k_resident2d<64>);
   set_attr((const void*)k_resident2d<128>);
   set_attr((const void*)k_resident2d<256>);
   set_attr((const void*)k_resident2d<512>);
-  set_attr((const void*)k_resident2d<1024>);
   for (int c = 0; c < kNumClasses; ++c) {
     if (!class_count_[c]) continue;
-    const std::size_t smem = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+    const void* k;
+    int threads;
+    if (c >= kGenericClasses) {
+      const FixedSpec& f = fixed_specs()[c - kGenericClasses];
+      k = fixed_kernel(c - kGenericClasses);
+      threads = f.nt;
+      class_smem_[c] = 3 * static_cast<std::size_t>(rf::padded(f.n)) * sizeof(cf);
+      set_attr(k);
+    } else {
+      k = c == 0 ? (const void*)k_resident2d<64> : c == 1 ? (const void*)k_resident2d<128>
+          : c == 2 ? (const void*)k_resident2d<256> : (const void*)k_resident2d<512>;
+      threads = kClassThreads[c];
+      class_smem_[c] = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+    }
     int per_sm = 0;
-    const void* k = c == 0 ? (const void*)k_resident2d<128> : c == 1 ? (const void*)k_resident2d<256>
-                   : c == 2 ? (const void*)k_resident2d<512> : (const void*)k_resident2d<1024>;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kClassThreads[c], smem), "occupancy");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, class_smem_[c]), "occupancy");
     per_sm = std::max(1, per_sm);
     class_grid_[c] = std::min(class_count_[c], per_sm * sms_);
+    class_threads_[c] = threads;
+    class_fn_[c] = k;
   }
   bytes_ = d_steps_.bytes() + d_passes_.bytes() + d_pids_.bytes() + d_iface_.bytes() +
            d_tables_.bytes() + d_twiddles_.bytes() + d_lines_.bytes() + d_src_.bytes() +
@@ -620,22 +680,31 @@ void Batch2DImpl::prepare() {
 void Batch2DImpl::launch_classes(cudaStream_t origin) {
   check_cuda(cudaMemsetAsync(d_queue_.ptr, 0, kNumClasses * sizeof(int), origin), "queue reset");
   check_cuda(cudaEventRecord(ev0_, origin), "event");
-  // largest class first: its items are the longest chains
-  for (int c = kNumClasses - 1; c >= 0; --c) {
-    if (!class_count_[c]) continue;
+  // longest chains first: classes in decreasing order of their first item's cost
+  std::vector<int> order;
+  for (int c = 0; c < kNumClasses; ++c)
+    if (class_count_[c]) order.push_back(c);
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    return items_[class_first_[a]].cost > items_[class_first_[b]].cost;
+  });
+  for (int c : order) {
     cudaStream_t s = streams_[c];
     check_cuda(cudaStreamWaitEvent(s, ev0_, 0), "wait");
-    const std::size_t smem = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
     const R2Item* items = d_items_.ptr + class_first_[c];
-    R2Shared sh{d_plans_.ptr, d_twiddles_.ptr};
-    const dim3 grid(class_grid_[c]);
+    int count = class_count_[c];
     int* q = d_queue_.ptr + c;
-    switch (c) {
-      case 0: launch(k_resident2d<128>, grid, dim3(128), smem, s, items, class_count_[c], q, sh); break;
-      case 1: launch(k_resident2d<256>, grid, dim3(256), smem, s, items, class_count_[c], q, sh); break;
-      case 2: launch(k_resident2d<512>, grid, dim3(512), smem, s, items, class_count_[c], q, sh); break;
-      default: launch(k_resident2d<1024>, grid, dim3(1024), smem, s, items, class_count_[c], q, sh);
+    const dim3 grid(class_grid_[c]), block(class_threads_[c]);
+    if (c >= kGenericClasses) {
+      const int n = fixed_specs()[c - kGenericClasses].n;
+      const Tw<float>* tw = d_twiddles_.ptr + plan_twbase_[n];
+      void* args[] = {&items, &count, &q, &tw};
+      check_cuda(cudaLaunchKernel(class_fn_[c], grid, block, args, class_smem_[c], s), "launch");
+    } else {
+      R2Shared sh{d_plans_.ptr, d_twiddles_.ptr};
+      void* args[] = {&items, &count, &q, &sh};
+      check_cuda(cudaLaunchKernel(class_fn_[c], grid, block, args, class_smem_[c], s), "launch");
     }
+    ++launches_;
     check_cuda(cudaEventRecord(class_done_[c], s), "event");
     check_cuda(cudaStreamWaitEvent(origin, class_done_[c], 0), "wait");
   }

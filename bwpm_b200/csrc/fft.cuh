@@ -196,7 +196,7 @@ __device__ __forceinline__ void dft(cx<T>* u) {
 // One stage of radix R on `batch` lanes (point stride `batch`), in place; a thread stages up to
 // EPT values (kmax_for(R, EPT) butterflies).
 template <int DIR, int R, int EPT, typename T>
-__device__ __forceinline__ void stage(cx<T>* buf, int n, int len, const Tw<T>* __restrict__ tw,
+__device__ __noinline__ void stage(cx<T>* buf, int n, int len, const Tw<T>* __restrict__ tw,
                                       int batch, int tid, int nthreads) {
   constexpr int K = kmax_for(R, EPT);
   const int nb = n / R;
@@ -213,9 +213,9 @@ __device__ __forceinline__ void stage(cx<T>* buf, int n, int len, const Tw<T>* _
 #pragma unroll
       for (int r = 0; r < R; ++r) u[k][r] = buf[(i + r * nb) * batch + b];
       if (len > 1) {
-        const Tw<T>* w = tw + kk * (R - 1);
+        // r-major layout: consecutive k (consecutive threads) read consecutive entries
 #pragma unroll
-        for (int r = 1; r < R; ++r) u[k][r] = twmul<DIR>(u[k][r], w[r - 1]);
+        for (int r = 1; r < R; ++r) u[k][r] = twmul<DIR>(u[k][r], tw[(r - 1) * len + kk]);
       }
       dft<DIR, R>(u[k]);
       dst[k] = ((i - kk) * R + kk) * batch + b;
@@ -248,7 +248,7 @@ __device__ __noinline__ void stage_generic(cx<T>* buf, int n, int len, int R,
     const int kk = i % len;
     for (int r = 0; r < R; ++r) u[r] = buf[(i + r * nb) * batch + b];
     if (len > 1)
-      for (int r = 1; r < R; ++r) u[r] = twmul<DIR>(u[r], tw[kk * (R - 1) + r - 1]);
+      for (int r = 1; r < R; ++r) u[r] = twmul<DIR>(u[r], tw[(r - 1) * len + kk]);
     const int step = n / R;  // roots[j·step] = exp(−2πi j/R)
     for (int m = 0; m < R; ++m) {
       cx<T> acc = u[0];

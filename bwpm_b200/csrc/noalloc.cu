@@ -55,7 +55,7 @@ __global__ void k_noalloc_twiddles(Tw<double>* tw, FftPlan plan) {
   while (s > 0 && plan.twoff[s] > i) --s;
   const int r = plan.radix[s], len = plan.len[s];
   const int local = i - plan.twoff[s];
-  const int k = local / (r - 1), j = local % (r - 1) + 1;
+  const int j = local / len + 1, k = local % len;  // r-major: entry (j − 1)·L + k
   const long long lr = static_cast<long long>(len) * r;
   const long long m = (static_cast<long long>(j) * k) % lr;
   double sn, cs;

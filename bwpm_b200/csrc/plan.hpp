@@ -52,11 +52,19 @@ inline std::vector<int> factorize(int n) {
   return r;
 }
 
-inline HostPlan make_plan(int n) {
+inline HostPlan make_plan_radices(int n, const std::vector<int>& radices);
+
+inline HostPlan make_plan(int n) { return make_plan_radices(n, n > 1 ? factorize(n) : std::vector<int>{}); }
+
+// Plan with a given radix order (the product must be n).
+inline HostPlan make_plan_radices(int n, const std::vector<int>& radices) {
   HostPlan hp;
   FftPlan& p = hp.plan;
   p.n = n;
-  const std::vector<int> radices = n > 1 ? factorize(n) : std::vector<int>{};
+  long long prod = 1;
+  for (int r : radices) prod *= r;
+  if (prod != n || static_cast<int>(radices.size()) > kMaxStages)
+    throw invalid_argument("radices do not factor the FFT length");
   p.nstages = static_cast<int>(radices.size());
   int len = 1, off = 0;
   const double two_pi = 6.283185307179586476925286766559;
@@ -66,8 +74,8 @@ inline HostPlan make_plan(int n) {
     p.len[s] = len;
     p.twoff[s] = off;
     const long long lr = static_cast<long long>(len) * r;
-    for (int k = 0; k < len; ++k)
-      for (int j = 1; j < r; ++j) {
+    for (int j = 1; j < r; ++j)  // r-major: entry (j − 1)·L + k
+      for (int k = 0; k < len; ++k) {
         const long long m = (static_cast<long long>(j) * k) % lr;
         const double a = -two_pi * static_cast<double>(m) / static_cast<double>(lr);
         hp.twiddles.push_back(cd{std::cos(a), std::sin(a)});

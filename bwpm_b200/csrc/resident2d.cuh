@@ -17,7 +17,7 @@
 
 namespace bwpm {
 
-constexpr int kR2Ept = 8;  // complex values a thread stages per FFT stage
+constexpr int kR2Ept = 16;  // complex values a thread stages per FFT stage
 
 struct R2Pass {
   long long tab;  // element offset of the scalar operator table: N hi values, then N lo values
@@ -223,6 +223,205 @@ __global__ void __launch_bounds__(NT) k_resident2d(const R2Item* __restrict__ it
     }
     __syncthreads();
     if (tid == 0) it.clock[1] = global_ns();
+    __syncthreads();
+  }
+}
+
+// ---- specialised kernels for compile-time lengths (register-resident lines) -----------------
+//
+// Same work items and results as k_resident2d, for one length N per launch: the field, the
+// spectrum of a multi-pass step and the output of the step stay in registers in the owned
+// pattern of rf::fft (position t + m·NT in register m of thread t); shared memory holds only the
+// two exchange buffers of the transform, which also serve the gather of reflection sources and
+// the sparse add at interface pixels.
+
+}  // namespace bwpm
+
+#include "rfft.cuh"
+
+namespace bwpm {
+
+template <int N, int NT>
+__device__ __forceinline__ void r2f_load(cf (&v)[N / NT], const cf* src, int t) {
+#pragma unroll
+  for (int m = 0; m < N / NT; ++m) v[m] = src[t + m * NT];
+}
+
+template <int N, int NT>
+__device__ __forceinline__ void r2f_store(cf* dst, const cf (&v)[N / NT], int t) {
+#pragma unroll
+  for (int m = 0; m < N / NT; ++m) dst[t + m * NT] = v[m];
+}
+
+// Σ w[q]·|v|² over the owned values, compensated in FP64; thread 0 returns the block total.
+template <int N, int NT>
+__device__ __forceinline__ double r2f_flux(const cf (&v)[N / NT], const double* w, double* red, int t) {
+  double s = 0.0, c = 0.0;
+#pragma unroll
+  for (int m = 0; m < N / NT; ++m) {
+    const double a = w[t + m * NT] * (static_cast<double>(v[m].re) * v[m].re +
+                                      static_cast<double>(v[m].im) * v[m].im);
+    const double y = a - c;
+    const double z = s + y;
+    c = (z - s) - y;
+    s = z;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((t & 31) == 0) red[t >> 5] = s;
+  __syncthreads();
+  double total = 0.0;
+  if (t == 0) {
+    double comp = 0.0;
+    for (int i = 0; i < NT / 32; ++i) {
+      const double y = red[i] - comp;
+      const double z = total + y;
+      comp = (z - total) - y;
+      total = z;
+    }
+  }
+  __syncthreads();
+  return total;
+}
+
+// The spectrum of a multi-pass step is kept in the shared line S at the owned positions (each
+// thread reads back only what it wrote, so S needs no barrier).
+template <int N, int NT, class RADS>
+__device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / NT],
+                                         cf* b0, cf* b1, int& phase, const R2Item& it,
+                                         const R2Step& st, bool backward, bool reflect, cf* store,
+                                         const cf* add, const Tw<float>* __restrict__ tw, int t) {
+  constexpr int E = N / NT;
+  const int off = backward ? st.bwd_off : st.fwd_off;
+  const int ntp = backward ? st.bwd_t : st.fwd_t;
+  const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
+  const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
+  const int* iface = it.iface + st.iface;
+  rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+  if (npass == 1) {  // one transmission pass over every pixel
+    const cf* m = it.tables + it.passes[off].tab;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const int q = t + k * NT;
+      v[k] = pmul(v[k], m[q], m[N + q]);
+      if ((k & 3) == 3) asm volatile("" ::: "memory");  // bound the loads in flight
+    }
+    rf::fft<+1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+    if (it.mask)
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        const int q = t + k * NT;
+        v[k] = mask_mul(v[k], it.mask[q], it.mask[N + q]);
+        if ((k & 3) == 3) asm volatile("" ::: "memory");
+      }
+  } else {
+#pragma unroll
+    for (int k = 0; k < E; ++k) S[rf::pad(t + k * NT)] = v[k];
+    for (int j = 0; j < npass; ++j) {
+      const R2Pass ps = it.passes[off + j];
+      const cf* m = it.tables + ps.tab;
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        const int q = t + k * NT;
+        v[k] = pmul(S[rf::pad(q)], m[q], m[N + q]);
+        if ((k & 3) == 3) asm volatile("" ::: "memory");
+      }
+      rf::fft<+1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+      if (!ps.refl) {
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+          const int q = t + k * NT;
+          if (!pid || pid[q] == ps.pair) out[k] = it.mask ? mask_mul(v[k], it.mask[q], it.mask[N + q]) : v[k];
+          if ((k & 3) == 3) asm volatile("" ::: "memory");
+        }
+      } else {  // gather at the interface pixels through the free exchange buffer
+        cf* buf = phase ? b1 : b0;
+#pragma unroll
+        for (int k = 0; k < E; ++k) buf[rf::pad(t + k * NT)] = v[k];
+        __syncthreads();
+        for (int k = t; k < st.niface; k += NT) {
+          const int q = iface[k];
+          if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q)];
+        }
+        phase ^= 1;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) v[k] = out[k];
+  }
+  if (add) {  // sparse sources of the other pass at this step's interface pixels
+    cf* buf = phase ? b1 : b0;
+#pragma unroll
+    for (int k = 0; k < E; ++k) buf[rf::pad(t + k * NT)] = v[k];
+    __syncthreads();
+    for (int k = t; k < st.niface; k += NT) {
+      const int q = rf::pad(iface[k]);
+      buf[q] = buf[q] + add[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < E; ++k) v[k] = buf[rf::pad(t + k * NT)];
+    phase ^= 1;
+  }
+}
+
+template <int N, int NT, class RADS>
+__global__ void __launch_bounds__(NT) k_resident2d_fixed(const R2Item* __restrict__ items,
+                                                         int nitems, int* queue,
+                                                         const Tw<float>* __restrict__ tw) {
+  constexpr int E = N / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cf* b0 = reinterpret_cast<cf*>(smem_raw);
+  cf* b1 = b0 + rf::padded(N);
+  cf* S = b1 + rf::padded(N);
+  __shared__ int s_item;
+  __shared__ double s_red[NT / 32];
+  const int t = threadIdx.x;
+  int phase = 0;
+  for (;;) {
+    if (t == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int idx = s_item;
+    if (idx >= nitems) return;
+    const R2Item it = items[idx];
+    if (t == 0) it.clock[0] = global_ns();
+    cf v[E], out[E];
+    const int iters = it.iterations > 0 ? it.iterations : 1;
+    r2f_load<N, NT>(v, it.input, t);
+    rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+    {
+      const double pin = r2f_flux<N, NT>(v, it.w_in, s_red, t);
+      if (t == 0) it.energy[2 * iters] = pin;
+    }
+    // sweeps alternate forward (even) and backward (odd); iterations = 0: one forward sweep
+    const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
+    for (int sw = 0; sw < sweeps; ++sw) {
+      const bool backward = sw & 1;
+      const int iter = sw >> 1;
+      if (!backward) {
+        r2f_load<N, NT>(v, it.input, t);
+      } else {
+#pragma unroll
+        for (int k = 0; k < E; ++k) v[k] = cf{0.f, 0.f};
+      }
+      for (int s = 0; s < it.nz; ++s) {
+        const int p = backward ? it.nz - 1 - s : s;  // step p: planes p and p + 1
+        const R2Step st = it.steps[p];
+        const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
+        const bool has_add = st.niface > 0 && (backward || iter > 0);
+        cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
+        const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
+        r2f_step<N, NT, RADS>(v, S, out, b0, b1, phase, it, st, backward, reflect, store, add, tw, t);
+      }
+      r2f_store<N, NT>(backward ? it.reflected : it.transmitted, v, t);
+      if (it.iterations == 0) break;
+#pragma unroll
+      for (int k = 0; k < E; ++k) out[k] = v[k];
+      rf::fft<-1, N, NT>(out, b0, b1, phase, tw, t, RADS{});
+      const double flux = r2f_flux<N, NT>(out, backward ? it.w_in : it.w_out, s_red, t);
+      if (t == 0) it.energy[2 * iter + (backward ? 1 : 0)] = flux;
+    }
+    __syncthreads();
+    if (t == 0) it.clock[1] = global_ns();
     __syncthreads();
   }
 }
