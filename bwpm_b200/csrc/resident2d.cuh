@@ -365,7 +365,7 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
 }
 
 template <int N, int NT, class RADS>
-__global__ void __launch_bounds__(NT) k_resident2d_fixed(const R2Item* __restrict__ items,
+__global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __restrict__ items,
                                                          int nitems, int* queue,
                                                          const Tw<float>* __restrict__ tw) {
   constexpr int E = N / NT;
