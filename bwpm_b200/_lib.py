@@ -50,6 +50,15 @@ SIGNATURES: dict[str, tuple] = {
     "bwpm_batch_stats": (_i, [_p, _i64p, _i64p, _i64p, _i64p, _i64p]),
     "bwpm_batch_work": (_i, [_p, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d)]),
     "bwpm_batch_destroy": (None, [_p]),
+    "bwpm_server_create": (_i, [_i, ctypes.c_uint64, _i, _i, _i, ctypes.POINTER(_p)]),
+    "bwpm_server_submit_2d": (_i, [_p, _sz, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _p, _i,
+                                   _i64p]),
+    "bwpm_server_submit_3d": (_i, [_p, _sz, _sz, _d, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _p,
+                                   _i, _i64p]),
+    "bwpm_server_wait": (_i, [_p, ctypes.c_int64, _d, ctypes.POINTER(_i)]),
+    "bwpm_server_result": (_i, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "bwpm_server_stats": (_i, [_p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
+    "bwpm_server_destroy": (None, [_p]),
     "bwpm_flush_l2": (_i, [_i, _sz]),
     "bwpm_step2d_noalloc": (_i, [_i, _sz, _d, _d, _d, _p, _sz, _p, _p, _d, _d, _p, _p, _p, _p]),
     "bwpm_host_register": (_i, [_p, _sz]),

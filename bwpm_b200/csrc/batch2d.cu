@@ -131,7 +131,11 @@ __global__ void k_pack_outputs(const ItemIo* io, cd* out) {
   }
 }
 
-struct HostSolve {
+}  // namespace
+
+// One solve with its host-side records (validated, pairs, pair ids, interface lists, passes);
+// built by prepare_solve() off the launch path, added to a batch by add_prepared().
+struct PreparedSolve {
   Solve2D in;
   // offsets into the pools
   long long step_base = 0, pass_base = 0, pid_base = 0, iface_base = 0, table_base = 0;
@@ -143,44 +147,81 @@ struct HostSolve {
   std::vector<int> iface;
   std::vector<std::tuple<int, cd, cd>> tables;  // (kind, ñ_r, ñ_s) per table slot
   int items[2] = {-1, -1};
+  bool built = false;  // host records built
 };
+
+namespace {
+using HostSolve = PreparedSolve;
 
 struct Item {
   int solve, comp, cls, n;
   double cost;
 };
 
+void validate2d(const Solve2D& s) {
+  if (s.ny < 2) throw invalid_argument("ny must be >= 2");
+  if (s.nz < 1) throw invalid_argument("nz must be >= 1");
+  if (s.labels.size() != static_cast<std::size_t>(s.nz) * s.ny)
+    throw invalid_argument("labels must have shape (nz, ny)");
+  if (!s.mask.empty() && s.mask.size() != static_cast<std::size_t>(s.ny))
+    throw invalid_argument("mask must have shape (ny,)");
+  if (s.field.size() != static_cast<std::size_t>(2 * s.ny)) throw invalid_argument("field must have shape (ny, 2)");
+  if (s.iterations < 0) throw invalid_argument("iterations must be >= 0");
+  for (auto l : s.labels)
+    if (l < 0 || static_cast<std::size_t>(l) >= s.indices.size())
+      throw invalid_argument("labels must index into `indices`");
+  if (s.indices.size() > 255) throw invalid_argument("at most 255 materials per 2D solve");
+  if (3 * static_cast<std::size_t>(s.ny) * sizeof(cf) > 220 * 1024)
+    throw invalid_argument("ny too large for the resident 2D engine (max 9216)");
+}
+
 class Batch2DImpl final : public Batch2D {
  public:
   explicit Batch2DImpl(int device) : device_(device) {
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    keep_pool_memory(device);
     for (auto& s : streams_) check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
-    check_cuda(cudaStreamCreateWithFlags(&main_, cudaStreamNonBlocking), "stream");
-    check_cuda(cudaEventCreate(&ev0_), "event");
-    check_cuda(cudaEventCreate(&ev1_), "event");
+    main_.create();
+    check_cuda(cudaEventCreateWithFlags(&ev0_, cudaEventDisableTiming), "event");
+    check_cuda(cudaEventCreate(&ev_start_), "event");
+    check_cuda(cudaEventCreate(&ev_stop_), "event");
+    check_cuda(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "event");
     for (auto& e : class_done_) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
     cudaDeviceProp prop{};
     check_cuda(cudaGetDeviceProperties(&prop, device), "props");
     sms_ = prop.multiProcessorCount;
   }
   ~Batch2DImpl() override {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (exec_packed_) cudaGraphExecDestroy(exec_packed_);
+    cudaStreamSynchronize(main_);
     for (auto& s : streams_) cudaStreamDestroy(s);
-    cudaStreamDestroy(main_);
     cudaEventDestroy(ev0_);
-    cudaEventDestroy(ev1_);
+    cudaEventDestroy(ev_start_);
+    cudaEventDestroy(ev_stop_);
+    cudaEventDestroy(done_);
     for (auto& e : class_done_) cudaEventDestroy(e);
   }
 
   std::int64_t add(Solve2D s) override {
     if (prepared_) throw invalid_argument("batch already prepared");
-    validate(s);
+    validate2d(s);
     HostSolve h;
     h.in = std::move(s);
     solves_.push_back(std::move(h));
     return static_cast<std::int64_t>(solves_.size()) - 1;
   }
+  std::int64_t add_prepared(std::shared_ptr<PreparedSolve> p) override {
+    if (prepared_) throw invalid_argument("batch already prepared");
+    if (!p || !p->built) throw invalid_argument("solve not prepared");
+    solves_.push_back(std::move(*p));
+    return static_cast<std::int64_t>(solves_.size()) - 1;
+  }
 
   void prepare() override;
+  void set_graphs(bool on) override { use_graphs_ = on; }
+  void enqueue() override;
+  bool ready() override;
   float run() override;
   float solve_packed(const cd* fields, cd* out) override;
   void result(std::int64_t id, Solve2DResult& r) override;
@@ -200,24 +241,9 @@ class Batch2DImpl final : public Batch2D {
   }
 
  private:
-  static void validate(const Solve2D& s) {
-    if (s.ny < 2) throw invalid_argument("ny must be >= 2");
-    if (s.nz < 1) throw invalid_argument("nz must be >= 1");
-    if (s.labels.size() != static_cast<std::size_t>(s.nz) * s.ny)
-      throw invalid_argument("labels must have shape (nz, ny)");
-    if (!s.mask.empty() && s.mask.size() != static_cast<std::size_t>(s.ny))
-      throw invalid_argument("mask must have shape (ny,)");
-    if (s.field.size() != static_cast<std::size_t>(2 * s.ny)) throw invalid_argument("field must have shape (ny, 2)");
-    if (s.iterations < 0) throw invalid_argument("iterations must be >= 0");
-    for (auto l : s.labels)
-      if (l < 0 || static_cast<std::size_t>(l) >= s.indices.size())
-        throw invalid_argument("labels must index into `indices`");
-    if (s.indices.size() > 255) throw invalid_argument("at most 255 materials per 2D solve");
-    if (3 * static_cast<std::size_t>(s.ny) * sizeof(cf) > 220 * 1024)
-      throw invalid_argument("ny too large for the resident 2D engine (max 9216)");
-  }
-  void prepare_solve(HostSolve& h);
   void launch_classes(cudaStream_t origin);
+  void capture_graphs();
+  void download();
   template <typename K, typename... A>
   void launch(K kernel, dim3 grid, dim3 block, std::size_t smem, cudaStream_t s, A... args) {
     kernel<<<grid, block, smem, s>>>(args...);
@@ -226,13 +252,15 @@ class Batch2DImpl final : public Batch2D {
   }
 
   int device_;
+  OwnedStream main_;  // first: the pools below are stream-ordered allocations on it
   int sms_ = 148;
   bool prepared_ = false;
   std::vector<HostSolve> solves_;
   std::vector<Item> items_;
   cudaStream_t streams_[kNumClasses] = {};
-  cudaStream_t main_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr, exec_packed_ = nullptr;
+  int graph_kernels_ = 0, graph_packed_kernels_ = 0;
+  cudaEvent_t ev0_ = nullptr, ev_start_ = nullptr, ev_stop_ = nullptr, done_ = nullptr;
   cudaEvent_t class_done_[kNumClasses] = {};
   int class_count_[kNumClasses] = {};
   int class_first_[kNumClasses] = {};
@@ -259,6 +287,11 @@ class Batch2DImpl final : public Batch2D {
   DevBuf<ItemIo> d_io_;
   DevBuf<cd> d_packed_in_, d_packed_out_;
   std::vector<R2Item> h_items_;
+  std::vector<cf> h_lines_;
+  std::vector<double> h_energy_;
+  std::vector<long long> h_clock_;
+  bool downloaded_ = false;
+  bool use_graphs_ = true;
   std::vector<long long> item_energy_off_;
   long long packed_total_ = 0;
   std::size_t bytes_ = 0;
@@ -266,7 +299,7 @@ class Batch2DImpl final : public Batch2D {
   double work_transforms_ = 0, work_flops_ = 0, work_bytes_ = 0;
 };
 
-void Batch2DImpl::prepare_solve(HostSolve& h) {
+void build_host(HostSolve& h) {
   const Solve2D& s = h.in;
   const int n = s.ny;
   auto index_of = [&](int l) { return l < 0 ? s.index_before : s.indices[static_cast<std::size_t>(l)]; };
@@ -357,6 +390,7 @@ void Batch2DImpl::prepare_solve(HostSolve& h) {
     h.steps[p] = st;
   }
   h.iface_count = static_cast<long long>(h.iface.size());
+  h.built = true;
 }
 
 void Batch2DImpl::prepare() {
@@ -372,7 +406,7 @@ void Batch2DImpl::prepare() {
     for (unsigned t = 0; t < hw; ++t)
       pool.emplace_back([&, t] {
         try {
-          for (std::size_t i = next++; i < solves_.size(); i = next++) prepare_solve(solves_[i]);
+          for (std::size_t i = next++; i < solves_.size(); i = next++) if (!solves_[i].built) build_host(solves_[i]);
         } catch (...) {
           errs[t] = std::current_exception();
         }
@@ -518,36 +552,33 @@ void Batch2DImpl::prepare() {
       moff += 2LL * h.in.ny;
     }
   }
-  d_steps_.alloc(nsteps);
+  d_steps_.alloc(nsteps, main_);
   d_steps_.upload(steps.data(), nsteps);
-  d_passes_.alloc(std::max<long long>(npass, 1));
+  d_passes_.alloc(std::max<long long>(npass, 1), main_);
   d_passes_.upload(passes.data(), npass);
-  d_pids_.alloc(std::max<long long>(npid, 1));
+  d_pids_.alloc(std::max<long long>(npid, 1), main_);
   d_pids_.upload(pids.data(), npid);
-  d_iface_.alloc(std::max<long long>(niface, 1));
+  d_iface_.alloc(std::max<long long>(niface, 1), main_);
   d_iface_.upload(iface.data(), niface);
-  d_mask_.alloc(std::max<long long>(nmask, 1));
+  d_mask_.alloc(std::max<long long>(nmask, 1), main_);
   d_mask_.upload(mask.data(), nmask);
-  d_tables_.alloc(std::max<long long>(ntab, 1));
-  d_twiddles_.alloc(tw.size());
+  d_tables_.alloc(std::max<long long>(ntab, 1), main_);
+  d_twiddles_.alloc(tw.size(), main_);
   d_twiddles_.upload(tw.data(), tw.size());
-  d_plans_.alloc(plans.size());
+  d_plans_.alloc(plans.size(), main_);
   d_plans_.upload(plans.data(), plans.size());
-  d_lines_.alloc(nlines);
-  d_src_.alloc(std::max<long long>(nsrc, 1));
-  d_weights_.alloc(nweights);
-  d_energy_.alloc(nenergy);
-  d_clock_.alloc(2 * items_.size());
-  d_items_.alloc(items_.size());
-  d_queue_.alloc(kNumClasses);
-  d_io_.alloc(items_.size());
-  d_packed_in_.alloc(packed_total_);
-  d_packed_out_.alloc(2 * packed_total_);
-  check_cuda(cudaMemset(d_src_.ptr, 0, d_src_.bytes()), "memset");
-  check_cuda(cudaMemset(d_lines_.ptr, 0, d_lines_.bytes()), "memset");
-  // the uploads and memsets above run on the legacy default stream, which the non-blocking
-  // stream main_ does not wait for: finish them before any kernel on main_ touches the pools
-  check_cuda(cudaDeviceSynchronize(), "pool uploads");
+  d_lines_.alloc(nlines, main_);
+  d_src_.alloc(std::max<long long>(nsrc, 1), main_);
+  d_weights_.alloc(nweights, main_);
+  d_energy_.alloc(nenergy, main_);
+  d_clock_.alloc(2 * items_.size(), main_);
+  d_items_.alloc(items_.size(), main_);
+  d_queue_.alloc(kNumClasses, main_);
+  d_io_.alloc(items_.size(), main_);
+  d_packed_in_.alloc(packed_total_, main_);
+  d_packed_out_.alloc(2 * packed_total_, main_);
+  d_src_.zero();
+  d_lines_.zero();
   // operator tables (FP64 on the device, stored as complex64)
   std::vector<TableJob> tjobs;
   for (auto& h : solves_)
@@ -600,11 +631,9 @@ void Batch2DImpl::prepare() {
   }
   d_items_.upload(h_items_.data(), h_items_.size());
   d_io_.upload(io.data(), io.size());
-  check_cuda(cudaDeviceSynchronize(), "item uploads");
   if (!tjobs.empty()) {
-    DevBuf<TableJob> dj(tjobs.size());
+    DevBuf<TableJob> dj(tjobs.size(), main_);
     dj.upload(tjobs.data(), tjobs.size());
-    check_cuda(cudaDeviceSynchronize(), "job upload");
     int maxn = 0;
     for (auto& j : tjobs) maxn = std::max(maxn, j.n);
     for (std::size_t b = 0; b < tjobs.size(); b += 60000) {
@@ -614,9 +643,8 @@ void Batch2DImpl::prepare() {
     check_cuda(cudaStreamSynchronize(main_), "tables");
   }
   {
-    DevBuf<WeightJob> dj(wjobs.size());
+    DevBuf<WeightJob> dj(wjobs.size(), main_);
     dj.upload(wjobs.data(), wjobs.size());
-    check_cuda(cudaDeviceSynchronize(), "job upload");
     int maxn = 0;
     for (auto& j : wjobs) maxn = std::max(maxn, j.n);
     for (std::size_t b = 0; b < wjobs.size(); b += 60000) {
@@ -629,7 +657,6 @@ void Batch2DImpl::prepare() {
   std::vector<cd> packed(packed_total_);
   for (auto& h : solves_) std::copy(h.in.field.begin(), h.in.field.end(), packed.begin() + h.packed);
   d_packed_in_.upload(packed.data(), packed.size());
-  check_cuda(cudaDeviceSynchronize(), "input upload");
   launch(k_unpack_inputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
          (const ItemIo*)d_io_.ptr, (const cd*)d_packed_in_.ptr);
   check_cuda(cudaStreamSynchronize(main_), "inputs");
@@ -675,6 +702,7 @@ void Batch2DImpl::prepare() {
     std::vector<R2Pass>().swap(h.passes);
   }
   prepared_ = true;
+  if (use_graphs_) capture_graphs();
 }
 
 void Batch2DImpl::launch_classes(cudaStream_t origin) {
@@ -710,51 +738,107 @@ void Batch2DImpl::launch_classes(cudaStream_t origin) {
   }
 }
 
+void Batch2DImpl::capture_graphs() {
+  // one graph per entry point: the persistent class kernels (forked onto their streams and
+  // joined back), and for the packed end-to-end path unpack + classes + pack around them
+  auto capture = [&](bool packed, cudaGraphExec_t& exec, int& kernels) {
+    const std::int64_t before = launches_;
+    cudaGraph_t g;
+    check_cuda(cudaStreamBeginCapture(main_, cudaStreamCaptureModeThreadLocal), "capture");
+    if (packed)
+      launch(k_unpack_inputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+             (const ItemIo*)d_io_.ptr, (const cd*)d_packed_in_.ptr);
+    launch_classes(main_);
+    if (packed) {
+      check_cuda(cudaMemsetAsync(d_packed_out_.ptr, 0, d_packed_out_.bytes(), main_), "memset");
+      launch(k_pack_outputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+             (const ItemIo*)d_io_.ptr, d_packed_out_.ptr);
+    }
+    check_cuda(cudaStreamEndCapture(main_, &g), "capture");
+    check_cuda(cudaGraphInstantiate(&exec, g, 0), "instantiate");
+    cudaGraphDestroy(g);
+    kernels = static_cast<int>(launches_ - before);
+    launches_ = before;
+  };
+  capture(false, exec_, graph_kernels_);
+  capture(true, exec_packed_, graph_packed_kernels_);
+}
+
+void Batch2DImpl::enqueue() {
+  if (!prepared_) prepare();
+  check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+  if (exec_) {
+    check_cuda(cudaGraphLaunch(exec_, main_), "graph launch");
+    launches_ += graph_kernels_;
+  } else {
+    launch_classes(main_);
+  }
+  check_cuda(cudaEventRecord(done_, main_), "event");
+  downloaded_ = false;
+}
+
+bool Batch2DImpl::ready() {
+  const cudaError_t e = cudaEventQuery(done_);
+  if (e == cudaErrorNotReady) return false;
+  check_cuda(e, "batch");
+  return true;
+}
+
 float Batch2DImpl::run() {
   if (!prepared_) prepare();
   check_cuda(cudaSetDevice(device_), "cudaSetDevice");
-  cudaEvent_t start, stop;
-  check_cuda(cudaEventCreate(&start), "event");
-  check_cuda(cudaEventCreate(&stop), "event");
-  check_cuda(cudaEventRecord(start, main_), "event");
-  launch_classes(main_);
-  check_cuda(cudaEventRecord(stop, main_), "event");
-  check_cuda(cudaEventSynchronize(stop), "run");
+  check_cuda(cudaEventRecord(ev_start_, main_), "event");
+  enqueue();
+  check_cuda(cudaEventRecord(ev_stop_, main_), "event");
+  check_cuda(cudaEventSynchronize(ev_stop_), "run");
   float ms = 0;
-  check_cuda(cudaEventElapsedTime(&ms, start, stop), "elapsed");
-  cudaEventDestroy(start);
-  cudaEventDestroy(stop);
+  check_cuda(cudaEventElapsedTime(&ms, ev_start_, ev_stop_), "elapsed");
   return ms;
 }
 
 float Batch2DImpl::solve_packed(const cd* fields, cd* out) {
   if (!prepared_) prepare();
   check_cuda(cudaSetDevice(device_), "cudaSetDevice");
-  cudaEvent_t start, stop;
-  check_cuda(cudaEventCreate(&start), "event");
-  check_cuda(cudaEventCreate(&stop), "event");
-  check_cuda(cudaEventRecord(start, main_), "event");
+  check_cuda(cudaEventRecord(ev_start_, main_), "event");
   check_cuda(cudaMemcpyAsync(d_packed_in_.ptr, fields, packed_total_ * sizeof(cd), cudaMemcpyHostToDevice, main_), "h2d");
-  launch(k_unpack_inputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
-         (const ItemIo*)d_io_.ptr, (const cd*)d_packed_in_.ptr);
-  launch_classes(main_);
-  check_cuda(cudaMemsetAsync(d_packed_out_.ptr, 0, d_packed_out_.bytes(), main_), "memset");
-  launch(k_pack_outputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
-         (const ItemIo*)d_io_.ptr, d_packed_out_.ptr);
+  if (exec_packed_) {
+    check_cuda(cudaGraphLaunch(exec_packed_, main_), "graph launch");
+    launches_ += graph_packed_kernels_;
+  } else {
+    launch(k_unpack_inputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+           (const ItemIo*)d_io_.ptr, (const cd*)d_packed_in_.ptr);
+    launch_classes(main_);
+    check_cuda(cudaMemsetAsync(d_packed_out_.ptr, 0, d_packed_out_.bytes(), main_), "memset");
+    launch(k_pack_outputs, dim3(8, static_cast<unsigned>(items_.size())), dim3(256), 0, main_,
+           (const ItemIo*)d_io_.ptr, d_packed_out_.ptr);
+  }
   check_cuda(cudaMemcpyAsync(out, d_packed_out_.ptr, 2 * packed_total_ * sizeof(cd), cudaMemcpyDeviceToHost, main_), "d2h");
-  check_cuda(cudaEventRecord(stop, main_), "event");
-  check_cuda(cudaEventSynchronize(stop), "solve");
+  check_cuda(cudaEventRecord(ev_stop_, main_), "event");
+  check_cuda(cudaEventRecord(done_, main_), "event");
+  check_cuda(cudaEventSynchronize(ev_stop_), "solve");
+  downloaded_ = false;
   float ms = 0;
-  check_cuda(cudaEventElapsedTime(&ms, start, stop), "elapsed");
-  cudaEventDestroy(start);
-  cudaEventDestroy(stop);
+  check_cuda(cudaEventElapsedTime(&ms, ev_start_, ev_stop_), "elapsed");
   return ms;
+}
+
+void Batch2DImpl::download() {
+  if (downloaded_) return;
+  check_cuda(cudaSetDevice(device_), "cudaSetDevice");
+  h_lines_.resize(d_lines_.n);
+  h_energy_.resize(d_energy_.n);
+  h_clock_.resize(d_clock_.n);
+  check_cuda(cudaMemcpyAsync(h_lines_.data(), d_lines_.ptr, d_lines_.bytes(), cudaMemcpyDeviceToHost, main_), "d2h");
+  check_cuda(cudaMemcpyAsync(h_energy_.data(), d_energy_.ptr, d_energy_.bytes(), cudaMemcpyDeviceToHost, main_), "d2h");
+  check_cuda(cudaMemcpyAsync(h_clock_.data(), d_clock_.ptr, d_clock_.bytes(), cudaMemcpyDeviceToHost, main_), "d2h");
+  check_cuda(cudaStreamSynchronize(main_), "d2h");
+  downloaded_ = true;
 }
 
 void Batch2DImpl::result(std::int64_t id, Solve2DResult& r) {
   if (!prepared_) throw invalid_argument("batch not run");
   if (id < 0 || id >= static_cast<std::int64_t>(solves_.size())) throw invalid_argument("unknown solve id");
-  check_cuda(cudaStreamSynchronize(main_), "sync");
+  download();
   const HostSolve& h = solves_[id];
   const int n = h.in.ny;
   const int iters = std::max(1, h.in.iterations);
@@ -764,26 +848,22 @@ void Batch2DImpl::result(std::int64_t id, Solve2DResult& r) {
   r.flux_r.assign(h.in.iterations, 0.0);
   r.flux_in = 0.0;
   long long t0 = -1, t1 = -1;
-  std::vector<cf> line(n);
-  std::vector<double> en(2 * iters + 1);
   for (int c = 0; c < 2; ++c) {
     const int k = h.items[c];
     if (k < 0) continue;
     const R2Item& it = h_items_[k];
-    check_cuda(cudaMemcpy(line.data(), it.transmitted, n * sizeof(cf), cudaMemcpyDeviceToHost), "d2h");
-    for (int q = 0; q < n; ++q) r.transmitted[2 * q + c] = cast<double>(line[q]);
-    if (h.in.iterations > 0) {
-      check_cuda(cudaMemcpy(line.data(), it.reflected, n * sizeof(cf), cudaMemcpyDeviceToHost), "d2h");
-      for (int q = 0; q < n; ++q) r.reflected[2 * q + c] = cast<double>(line[q]);
-    }
-    check_cuda(cudaMemcpy(en.data(), it.energy, en.size() * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+    const cf* lt = h_lines_.data() + (it.transmitted - d_lines_.ptr);
+    const cf* lr = h_lines_.data() + (it.reflected - d_lines_.ptr);
+    for (int q = 0; q < n; ++q) r.transmitted[2 * q + c] = cast<double>(lt[q]);
+    if (h.in.iterations > 0)
+      for (int q = 0; q < n; ++q) r.reflected[2 * q + c] = cast<double>(lr[q]);
+    const double* en = h_energy_.data() + item_energy_off_[k];
     for (int i = 0; i < h.in.iterations; ++i) {
       r.flux_t[i] += en[2 * i];
       r.flux_r[i] += en[2 * i + 1];
     }
     r.flux_in += en[2 * iters];
-    long long clk[2];
-    check_cuda(cudaMemcpy(clk, it.clock, sizeof(clk), cudaMemcpyDeviceToHost), "d2h");
+    const long long* clk = h_clock_.data() + 2 * k;
     t0 = t0 < 0 ? clk[0] : std::min(t0, clk[0]);
     t1 = std::max(t1, clk[1]);
   }
@@ -793,5 +873,36 @@ void Batch2DImpl::result(std::int64_t id, Solve2DResult& r) {
 }  // namespace
 
 std::unique_ptr<Batch2D> make_batch2d(int device) { return std::make_unique<Batch2DImpl>(device); }
+
+std::shared_ptr<PreparedSolve> prepare_solve(Solve2D s) {
+  validate2d(s);
+  auto p = std::make_shared<PreparedSolve>();
+  p->in = std::move(s);
+  build_host(*p);
+  return p;
+}
+
+std::size_t prepared_device_bytes(const PreparedSolve& p) {
+  // the pools prepare() allocates for this solve (an upper bound: a batch shares the twiddles
+  // of equal lengths)
+  const Solve2D& s = p.in;
+  const std::size_t n = static_cast<std::size_t>(s.ny);
+  int items = 0;
+  for (int c = 0; c < 2; ++c)
+    for (std::size_t q = 0; q < n; ++q)
+      if (s.field[2 * q + c].re != 0.0 || s.field[2 * q + c].im != 0.0) {
+        ++items;
+        break;
+      }
+  const std::size_t iters = static_cast<std::size_t>(std::max(1, s.iterations));
+  std::size_t b = p.steps.size() * sizeof(R2Step) + p.passes.size() * sizeof(R2Pass) + p.pids.size() +
+                  p.iface.size() * sizeof(int) + p.tables.size() * 4 * n * sizeof(cf) +
+                  (s.mask.empty() ? 0 : 2 * n * sizeof(float)) + 6 * n * sizeof(cd) +
+                  n * sizeof(Tw<float>) + 64;  // twiddles of the length (shared within a batch)
+  b += static_cast<std::size_t>(items) *
+       (3 * n * sizeof(cf) + 2 * p.iface.size() * sizeof(cf) + 2 * n * sizeof(double) +
+        (2 * iters + 1) * sizeof(double) + 2 * sizeof(long long) + sizeof(R2Item) + sizeof(ItemIo));
+  return b;
+}
 
 }  // namespace bwpm

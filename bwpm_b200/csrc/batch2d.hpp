@@ -28,12 +28,26 @@ struct Solve2DResult {
   double latency_ms = 0;                   // device time from first CTA start to last CTA end
 };
 
+// One solve with its host-side records (validated; pairs, pair-id planes, interface lists and
+// passes per step), built off the launch path by prepare_solve().
+struct PreparedSolve;
+std::shared_ptr<PreparedSolve> prepare_solve(Solve2D s);  // throws std::invalid_argument
+// device memory a batch allocates for this solve
+std::size_t prepared_device_bytes(const PreparedSolve& p);
+
 class Batch2D {
  public:
   virtual ~Batch2D() = default;
   virtual std::int64_t add(Solve2D s) = 0;
+  virtual std::int64_t add_prepared(std::shared_ptr<PreparedSolve> p) = 0;
   // builds pools, tables, plans and launch shapes; called once after the last add
   virtual void prepare() = 0;
+  // off: no CUDA graphs are captured at prepare (single-use batches); default on
+  virtual void set_graphs(bool on) = 0;
+  // enqueues one batched solve on the batch's stream and returns at once; ready() tells whether
+  // it has finished (results then come from result())
+  virtual void enqueue() = 0;
+  virtual bool ready() = 0;
   // one batched solve of every added problem with inputs resident; returns device ms
   virtual float run() = 0;
   // end-to-end: uploads packed complex128 inputs (Σ ny·2 values, add order), runs, downloads

@@ -7,6 +7,7 @@
 #include "../../include/bwpm_b200.h"
 #include "batch2d.hpp"
 #include "noalloc.hpp"
+#include "server.hpp"
 #include "solver.hpp"
 
 struct bwpm_solver {
@@ -15,6 +16,10 @@ struct bwpm_solver {
 
 struct bwpm_batch {
   std::unique_ptr<bwpm::Batch2D> impl;
+};
+
+struct bwpm_server {
+  std::unique_ptr<bwpm::Server> impl;
 };
 
 namespace {
@@ -232,6 +237,122 @@ int bwpm_batch_work(const bwpm_batch* b, double* transforms, double* flops, doub
 }
 
 void bwpm_batch_destroy(bwpm_batch* b) { delete b; }
+
+int bwpm_server_create(int device, uint64_t budget_bytes, int max_groups, int max_group_solves,
+                       int max_3d, bwpm_server** out) {
+  return guarded([&] {
+    if (!out) throw bwpm::invalid_argument("null output");
+    bwpm::ServerOptions o;
+    o.device = device;
+    o.budget_bytes = static_cast<std::size_t>(budget_bytes);
+    if (max_groups > 0) o.max_groups = max_groups;
+    if (max_group_solves > 0) o.max_group_solves = max_group_solves;
+    if (max_3d > 0) o.max_3d = max_3d;
+    auto* s = new bwpm_server;
+    try {
+      s->impl = bwpm::make_server(o);
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+  });
+}
+
+int bwpm_server_submit_2d(bwpm_server* s, size_t ny, double dy, double dz, double k0,
+                          const double* indices, size_t m, const int32_t* labels, size_t nz,
+                          double ib_re, double ib_im, const double* mask, const double* field,
+                          int iterations, int64_t* ticket) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
+    bwpm::Solve2D p;
+    p.ny = static_cast<int>(ny);
+    p.nz = static_cast<int>(nz);
+    p.dy = dy;
+    p.dz = dz;
+    p.k0 = k0;
+    p.indices.assign(as_cd(indices), as_cd(indices) + m);
+    p.labels.assign(labels, labels + nz * ny);
+    p.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) p.mask.assign(mask, mask + ny);
+    p.field.assign(as_cd(field), as_cd(field) + 2 * ny);
+    p.iterations = iterations;
+    const int64_t k = s->impl->submit2d(std::move(p));
+    if (ticket) *ticket = k;
+  });
+}
+
+int bwpm_server_submit_3d(bwpm_server* s, size_t ny, size_t nx, double dy, double dx, double dz,
+                          double k0, const double* indices, size_t m, const int32_t* labels,
+                          size_t nz, double ib_re, double ib_im, const double* mask,
+                          const double* field, int iterations, int64_t* ticket) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
+    bwpm::SolverInput in;
+    in.ny = ny;
+    in.nx = nx;
+    in.dy = dy;
+    in.dx = dx;
+    in.dz = dz;
+    in.k0 = k0;
+    in.indices.assign(as_cd(indices), as_cd(indices) + m);
+    in.labels.assign(labels, labels + nz * ny * nx);
+    in.nz = nz;
+    in.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) in.mask.assign(mask, mask + ny * nx);
+    std::vector<bwpm::cd> f(as_cd(field), as_cd(field) + 2 * ny * nx);
+    const int64_t k = s->impl->submit3d(std::move(in), std::move(f), iterations);
+    if (ticket) *ticket = k;
+  });
+}
+
+int bwpm_server_wait(bwpm_server* s, int64_t ticket, double timeout_s, int* done) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    const bool d = s->impl->wait(ticket, timeout_s);
+    if (done) *done = d ? 1 : 0;
+  });
+}
+
+int bwpm_server_result(bwpm_server* s, int64_t ticket, double* transmitted, double* reflected,
+                       double* flux_t, double* flux_r, double* flux_in, double* latency_ms,
+                       double* queue_ms, double* device_ms) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    bwpm::ServedResult r;
+    s->impl->result(ticket, r);
+    if (transmitted) std::memcpy(transmitted, r.transmitted.data(), r.transmitted.size() * sizeof(bwpm::cd));
+    if (reflected) std::memcpy(reflected, r.reflected.data(), r.reflected.size() * sizeof(bwpm::cd));
+    if (flux_t) std::memcpy(flux_t, r.flux_t.data(), r.flux_t.size() * sizeof(double));
+    if (flux_r) std::memcpy(flux_r, r.flux_r.data(), r.flux_r.size() * sizeof(double));
+    if (flux_in) *flux_in = r.flux_in;
+    if (latency_ms) *latency_ms = r.latency_ms;
+    if (queue_ms) *queue_ms = r.queue_ms;
+    if (device_ms) *device_ms = r.device_ms;
+  });
+}
+
+int bwpm_server_stats(bwpm_server* s, int64_t* submitted, int64_t* completed, int64_t* failed,
+                      int64_t* groups, int64_t* bytes_in_flight, int64_t* peak_bytes,
+                      int64_t* kernel_launches, int64_t* max_concurrent) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    bwpm::ServerStats st;
+    s->impl->stats(st);
+    if (submitted) *submitted = st.submitted;
+    if (completed) *completed = st.completed;
+    if (failed) *failed = st.failed;
+    if (groups) *groups = st.groups;
+    if (bytes_in_flight) *bytes_in_flight = st.bytes_in_flight;
+    if (peak_bytes) *peak_bytes = st.peak_bytes;
+    if (kernel_launches) *kernel_launches = st.kernel_launches;
+    if (max_concurrent) *max_concurrent = st.max_concurrent;
+  });
+}
+
+void bwpm_server_destroy(bwpm_server* s) { delete s; }
 
 int bwpm_flush_l2(int device, size_t bytes) {
   return guarded([&] {

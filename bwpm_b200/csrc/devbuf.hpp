@@ -1,4 +1,9 @@
 // RAII device allocation.
+//
+// A buffer is either a plain cudaMalloc allocation or a stream-ordered one (cudaMallocAsync /
+// cudaFreeAsync on the owner's stream). Stream-ordered buffers never synchronise the device when
+// they are freed, so several solvers can allocate, run and free concurrently on one GPU; their
+// owner must keep the stream alive until the buffer is released (declare the stream first).
 #pragma once
 
 #include <utility>
@@ -11,34 +16,95 @@ template <typename U>
 struct DevBuf {
   U* ptr = nullptr;
   std::size_t n = 0;
+  cudaStream_t stream = nullptr;  // stream of a stream-ordered allocation
+  bool ordered = false;
   DevBuf() = default;
   explicit DevBuf(std::size_t count) { alloc(count); }
+  DevBuf(std::size_t count, cudaStream_t s) { alloc(count, s); }
   void alloc(std::size_t count) {
     release();
     n = count;
     if (count) check_cuda(cudaMalloc(&ptr, count * sizeof(U)), "cudaMalloc");
   }
+  void alloc(std::size_t count, cudaStream_t s) {
+    release();
+    n = count;
+    stream = s;
+    ordered = true;
+    if (count) check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&ptr), count * sizeof(U), s), "cudaMallocAsync");
+  }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+      if (ordered)
+        cudaFreeAsync(ptr, stream);
+      else
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     n = 0;
+    ordered = false;
+    stream = nullptr;
   }
   ~DevBuf() { release(); }
-  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), n(o.n) {
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), n(o.n), stream(o.stream), ordered(o.ordered) {
     o.ptr = nullptr;
     o.n = 0;
+    o.ordered = false;
+    o.stream = nullptr;
   }
   DevBuf& operator=(DevBuf&& o) noexcept {
     std::swap(ptr, o.ptr);
     std::swap(n, o.n);
+    std::swap(stream, o.stream);
+    std::swap(ordered, o.ordered);
     return *this;
   }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   std::size_t bytes() const { return n * sizeof(U); }
+  // Stream-ordered buffers copy on their stream and wait for that stream only (the host data may
+  // be released on return; other streams of the device keep running).
   void upload(const U* host, std::size_t count) {
-    if (count) check_cuda(cudaMemcpy(ptr, host, count * sizeof(U), cudaMemcpyHostToDevice), "upload");
+    if (!count) return;
+    if (ordered) {
+      check_cuda(cudaMemcpyAsync(ptr, host, count * sizeof(U), cudaMemcpyHostToDevice, stream), "upload");
+      check_cuda(cudaStreamSynchronize(stream), "upload");
+    } else
+      check_cuda(cudaMemcpy(ptr, host, count * sizeof(U), cudaMemcpyHostToDevice), "upload");
+  }
+  void zero() {
+    if (!n) return;
+    if (ordered)
+      check_cuda(cudaMemsetAsync(ptr, 0, bytes(), stream), "memset");
+    else
+      check_cuda(cudaMemset(ptr, 0, bytes()), "memset");
   }
 };
+
+// A non-blocking stream owned by a solver; declared before the solver's buffers so that it is
+// destroyed after them.
+struct OwnedStream {
+  cudaStream_t s = nullptr;
+  OwnedStream() = default;
+  void create() { check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate"); }
+  ~OwnedStream() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+  OwnedStream(const OwnedStream&) = delete;
+  OwnedStream& operator=(const OwnedStream&) = delete;
+  operator cudaStream_t() const { return s; }
+};
+
+// Keeps freed stream-ordered memory in the device's default pool (no return to the driver
+// between solves); process-local, set once per device.
+inline void keep_pool_memory(int device) {
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return;
+  unsigned long long keep = ~0ull;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+}
 
 }  // namespace bwpm

@@ -45,9 +45,7 @@ template <typename T>
 class PlaneSolver final : public Solver {
  public:
   explicit PlaneSolver(SolverInput in) : in_(std::move(in)) { setup(); }
-  ~PlaneSolver() override {
-    if (stream_) cudaStreamDestroy(stream_);
-  }
+  ~PlaneSolver() override = default;
 
   void run(const cd* field, int iterations, const std::int64_t* keep, std::size_t nkeep,
            RunOutputs& out) override;
@@ -90,7 +88,7 @@ class PlaneSolver final : public Solver {
   }
 
   SolverInput in_;
-  cudaStream_t stream_ = nullptr;
+  OwnedStream stream_;  // first: outlives the stream-ordered buffers below
   HostPlan hy_, hx_;
   DevBuf<Tw<T>> tw_y_, tw_x_;
   std::vector<StepInfo> steps_;
@@ -178,12 +176,13 @@ void PlaneSolver<T>::setup() {
     }
   }
   check_cuda(cudaSetDevice(in_.device), "cudaSetDevice");
-  check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  stream_.create();
+  keep_pool_memory(in_.device);
   hy_ = make_plan(static_cast<int>(in_.ny));
   hx_ = make_plan(static_cast<int>(in_.nx));
   auto upload_tw = [&](const HostPlan& hp, DevBuf<Tw<T>>& d) {
     const std::vector<Tw<T>> t = twiddles_for<T>(hp);
-    d.alloc(t.size());
+    d.alloc(t.size(), stream_);
     d.upload(t.data(), t.size());
   };
   upload_tw(hy_, tw_y_);
@@ -250,20 +249,18 @@ void PlaneSolver<T>::setup() {
   }
   iface_total_ = static_cast<long long>(iface_host.size());
   if (!pid_host.empty()) {
-    pid_pool_.alloc(pid_host.size());
-    check_cuda(cudaMemcpy(pid_pool_.ptr, pid_host.data(), pid_host.size(), cudaMemcpyHostToDevice), "pid");
+    pid_pool_.alloc(pid_host.size(), stream_);
+    pid_pool_.upload(pid_host.data(), pid_host.size());
   }
   if (!iface_host.empty()) {
-    iface_pool_.alloc(iface_host.size());
-    check_cuda(cudaMemcpy(iface_pool_.ptr, iface_host.data(), iface_host.size() * sizeof(int),
-                          cudaMemcpyHostToDevice), "iface");
-    src_fwd_.alloc(2 * iface_host.size());
-    src_bwd_.alloc(2 * iface_host.size());
+    iface_pool_.alloc(iface_host.size(), stream_);
+    iface_pool_.upload(iface_host.data(), iface_host.size());
+    src_fwd_.alloc(2 * iface_host.size(), stream_);
+    src_bwd_.alloc(2 * iface_host.size(), stream_);
   }
   if (!rowoff_host.empty()) {
-    rowoff_pool_.alloc(rowoff_host.size());
-    check_cuda(cudaMemcpy(rowoff_pool_.ptr, rowoff_host.data(), rowoff_host.size() * sizeof(int),
-                          cudaMemcpyHostToDevice), "rowoff");
+    rowoff_pool_.alloc(rowoff_host.size(), stream_);
+    rowoff_pool_.upload(rowoff_host.data(), rowoff_host.size());
   }
   if (!in_.mask.empty()) {  // FP32: hi values then lo values (mask = hi + lo)
     const bool pair = sizeof(T) != sizeof(double);
@@ -272,14 +269,14 @@ void PlaneSolver<T>::setup() {
       m[q] = static_cast<T>(in_.mask[q]);
       if (pair) m[nn + q] = static_cast<T>(in_.mask[q] - static_cast<double>(m[q]));
     }
-    mask_.alloc(m.size());
+    mask_.alloc(m.size(), stream_);
     mask_.upload(m.data(), m.size());
   }
-  input_.alloc(2 * nn);
-  e_.alloc(2 * nn);
-  next_.alloc(2 * nn);
-  spec_.alloc(2 * nn);
-  stage_.alloc(2 * nn);
+  input_.alloc(2 * nn, stream_);
+  e_.alloc(2 * nn, stream_);
+  next_.alloc(2 * nn, stream_);
+  spec_.alloc(2 * nn, stream_);
+  stage_.alloc(2 * nn, stream_);
   // launch shapes and shared-memory opt-in
   if (is2d()) {
     thr2d_ = std::max(64, threads_needed(hy_.plan, 1));
@@ -296,8 +293,8 @@ void PlaneSolver<T>::setup() {
     cols1_ = cols_shape(2, 1);
     cols2_ = cols_shape(2, 2);
     cols3_ = cols_shape(3, 1);
-    xbuf_.alloc(2 * nn);
-    work_.alloc(static_cast<std::size_t>(max_pass_) * 2 * nn);
+    xbuf_.alloc(2 * nn, stream_);
+    work_.alloc(static_cast<std::size_t>(max_pass_) * 2 * nn, stream_);
     for (auto k : {(const void*)k_rows_fft<-1, T>, (const void*)k_rows_fft<1, T>,
                    (const void*)k_cols_step<T>, (const void*)k_rows_select<T>,
                    (const void*)k_cols_fft<-1, T>, (const void*)k_cols_fft<1, T>})
@@ -308,28 +305,25 @@ void PlaneSolver<T>::setup() {
     for (auto& pr : steps_[p].pairs) table(kFwdT, index_of(pr.first), index_of(pr.second));
   // Born: potential V = 2ñ₀k₀²δn per host slab, full-plane source stores
   if (!hosts_.empty()) {
-    pot_.alloc(hosts_.size() * nn);
-    DevBuf<cd> dn(nn);
-    std::vector<cd> v(nn);
+    pot_.alloc(hosts_.size() * nn, stream_);
+    std::vector<C> vt(hosts_.size() * nn);
     for (std::size_t p = 0; p < in_.nz; ++p) {
       const int slot = host_of[p];
       if (slot < 0) continue;
       const cd scale = ((2.0 * hosts_[slot]) * in_.k0) * in_.k0;  // cpp/src/solver.cpp:241
-      for (std::size_t q = 0; q < nn; ++q) v[q] = scale * in_.fluct[p * nn + q];
-      std::vector<C> vt(nn);
-      for (std::size_t q = 0; q < nn; ++q) vt[q] = cast<T>(v[q]);
-      check_cuda(cudaMemcpy(pot_.ptr + slot * nn, vt.data(), nn * sizeof(C), cudaMemcpyHostToDevice), "potential");
+      for (std::size_t q = 0; q < nn; ++q) vt[slot * nn + q] = cast<T>(scale * in_.fluct[p * nn + q]);
     }
-    born_fwd_.alloc(hosts_.size() * 2 * nn);
-    born_bwd_.alloc(hosts_.size() * 2 * nn);
-    w3_.alloc(3 * nn);
-    t3_.alloc(3 * nn);
-    sources_.alloc(6 * nn);
-    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &inc_}) b->alloc(2 * nn);
-    partial_.alloc(1024);
+    pot_.upload(vt.data(), vt.size());
+    born_fwd_.alloc(hosts_.size() * 2 * nn, stream_);
+    born_bwd_.alloc(hosts_.size() * 2 * nn, stream_);
+    w3_.alloc(3 * nn, stream_);
+    t3_.alloc(3 * nn, stream_);
+    sources_.alloc(6 * nn, stream_);
+    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &inc_}) b->alloc(2 * nn, stream_);
+    partial_.alloc(1024, stream_);
     partial_host_.resize(1024);
   }
-  check_cuda(cudaDeviceSynchronize(), "setup");
+  check_cuda(cudaStreamSynchronize(stream_), "setup");  // this solver's stream only
 }
 
 template <typename T>
@@ -337,7 +331,7 @@ const cx<T>* PlaneSolver<T>::table(int kind, cd nr, cd ns) {
   auto key = std::make_tuple(kind, nr.re, nr.im, ns.re, ns.im);
   auto it = tables_.find(key);
   if (it != tables_.end()) return it->second.ptr;
-  DevBuf<C> t(table_blocks<T>() * n());
+  DevBuf<C> t(table_blocks<T>() * n(), stream_);
   launch(k_build_table<T>, dim3(ceil_div(n(), kThreads)), dim3(kThreads), 0, t.ptr, kind, nr, ns,
          static_cast<int>(in_.ny), static_cast<int>(in_.nx), in_.dy, in_.dx, in_.k0, in_.dz);
   const C* ptr = t.ptr;
@@ -494,7 +488,7 @@ void PlaneSolver<T>::gmres(int slot, int dir) {
   const int restart = 30;
   const double tol = in_.gmres_tol;
   if (basis_.empty())
-    for (int i = 0; i <= restart; ++i) basis_.emplace_back(static_cast<std::size_t>(m2));
+    for (int i = 0; i <= restart; ++i) basis_.emplace_back(static_cast<std::size_t>(m2), stream_);
   auto apply = [&](const C* v, C* av) {  // av = v − G v/2
     born_operator(v, g_tmp_.ptr, slot, dir);
     ++gmres_applies_;
@@ -625,10 +619,10 @@ void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* ke
   std::vector<int> keep_slot(nz + 1, -1);
   for (std::size_t i = 0; i < nkeep; ++i)
     if (keep[i] >= 0 && keep[i] <= nz) keep_slot[keep[i]] = static_cast<int>(i);
-  DevBuf<C> kept_f(nkeep * 2 * nn), kept_b(nkeep * 2 * nn), t_iter, r_iter;
+  DevBuf<C> kept_f(nkeep * 2 * nn, stream_), kept_b(nkeep * 2 * nn, stream_), t_iter, r_iter;
   if (iterations > 0) {
-    t_iter.alloc(iterations * 2 * nn);
-    r_iter.alloc(iterations * 2 * nn);
+    t_iter.alloc(iterations * 2 * nn, stream_);
+    r_iter.alloc(iterations * 2 * nn, stream_);
   }
   check_cuda(cudaMemcpyAsync(stage_.ptr, field, n2 * sizeof(cd), cudaMemcpyHostToDevice, stream_), "field upload");
   launch(k_convert<T, double>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, input_.ptr,

@@ -119,6 +119,51 @@ int bwpm_batch_work(const bwpm_batch* b, double* transforms, double* flops, doub
 
 void bwpm_batch_destroy(bwpm_batch* b);
 
+/* ---- served request loop (continuous batching; no counterpart in the reference, which solves
+ * one problem per CudaSolver.run call: cpp/src/solver_cuda.cu:729-853) ----------------------
+ * Requests are submitted at any time and return a ticket at once. 2D requests (the reference's
+ * 2D convention, src/bwpm/fast.py:120-142) are prepared on host worker threads, admitted in
+ * arrival order while the device-memory budget holds, and launched in groups on the batched
+ * resident engine; groups launched while others run share the GPU. 3D requests run through the
+ * complex64 plane engine on their own streams. budget_bytes 0: 80 % of the free device memory;
+ * max_groups / max_group_solves / max_3d ≤ 0: defaults (8, 64, 2). Destroying the server waits
+ * for every submitted request. */
+typedef struct bwpm_server bwpm_server;
+
+int bwpm_server_create(int device, uint64_t budget_bytes, int max_groups, int max_group_solves,
+                       int max_3d, bwpm_server** out);
+
+/* Same arguments as bwpm_batch_add; *ticket identifies the request. */
+int bwpm_server_submit_2d(bwpm_server* s, size_t ny, double dy, double dz, double k0,
+                          const double* indices, size_t m, const int32_t* labels, size_t nz,
+                          double index_before_re, double index_before_im, const double* mask,
+                          const double* field, int iterations, int64_t* ticket);
+
+/* Same arguments as bwpm_solver_create (precision 32) plus the field (ny·nx·2 complex) and the
+ * iteration count of bwpm_solver_run. */
+int bwpm_server_submit_3d(bwpm_server* s, size_t ny, size_t nx, double dy, double dx, double dz,
+                          double k0, const double* indices, size_t m, const int32_t* labels,
+                          size_t nz, double index_before_re, double index_before_im,
+                          const double* mask, const double* field, int iterations,
+                          int64_t* ticket);
+
+/* Waits up to timeout_s seconds (< 0: without limit); *done = 1 when the request finished. */
+int bwpm_server_wait(bwpm_server* s, int64_t ticket, double timeout_s, int* done);
+
+/* Results of a finished request, then releases it: transmitted/reflected (ny·nx·2 complex),
+ * 2D only: flux_t/flux_r (iterations values) and flux_in; latency (submit → result), queueing
+ * (submit → launch) and device time in ms. A failed request returns its error. Pointers may be
+ * NULL. */
+int bwpm_server_result(bwpm_server* s, int64_t ticket, double* transmitted, double* reflected,
+                       double* flux_t, double* flux_r, double* flux_in, double* latency_ms,
+                       double* queue_ms, double* device_ms);
+
+int bwpm_server_stats(bwpm_server* s, int64_t* submitted, int64_t* completed, int64_t* failed,
+                      int64_t* groups, int64_t* bytes_in_flight, int64_t* peak_bytes,
+                      int64_t* kernel_launches, int64_t* max_concurrent);
+
+void bwpm_server_destroy(bwpm_server* s);
+
 /* Writes `bytes` of scratch memory on `device` (evicts the 126 MB L2 between timed runs). */
 int bwpm_flush_l2(int device, size_t bytes);
 
