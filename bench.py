@@ -230,6 +230,7 @@ def run_ours(args) -> None:
     params = _params()
     t_setup = time.perf_counter()
     b = Batch2D(device)
+    b.set_autotune(True)  # kernel variant per length chosen by measurement at prepare
     fields = []
     for prm in params:
         p = workloads.tilted_slab2d_from(prm)
@@ -311,7 +312,9 @@ def run_ours(args) -> None:
         "config": {"workload": WORKLOAD if not REDUCED else f"REDUCED profiling case {REDUCED}",
                    "global_batch": count * ws, "seq_len": None,
                    "parallelism": f"replicas{ws}", "l2": "flushed (512 MB write) before each timed step",
-                   "work_items": stats["work_items"], "classes": stats["classes"]},
+                   "work_items": stats["work_items"], "classes": stats["classes"],
+                   "kernels": [f"{c['ny']}:{c['threads']}t x{c['cluster']} v{c['variant']}"
+                               for c in b.classes()]},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "fp64_plain": {"value": fp64_rate, "unit": "solves/s", "sample": len(sample),
                        "note": "per-solve FP64 CudaSolver (drop-in path), mean sample time scaled "

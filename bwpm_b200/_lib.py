@@ -43,6 +43,11 @@ SIGNATURES: dict[str, tuple] = {
     "bwpm_solver_destroy": (None, [_p]),
     "bwpm_batch_create": (_i, [_i, ctypes.POINTER(_p)]),
     "bwpm_batch_add": (_i, [_p, _sz, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _p, _i, _i64p]),
+    "bwpm_batch_set_autotune": (_i, [_p, _i]),
+    "bwpm_batch_set_variant": (_i, [_p, _sz, _i]),
+    "bwpm_batch_class_info": (_i, [_p, ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, _i64p,
+                                   ctypes.POINTER(ctypes.c_float)]),
+    "bwpm_variant_count": (_i, [_sz]),
     "bwpm_batch_prepare": (_i, [_p]),
     "bwpm_batch_run": (_i, [_p, ctypes.POINTER(ctypes.c_float)]),
     "bwpm_batch_solve_packed": (_i, [_p, _p, _p, ctypes.POINTER(ctypes.c_float)]),

@@ -60,6 +60,26 @@ class Batch2D:
         return self.add(prob.ny, prob.dy, prob.dz, prob.k0, prob.indices, prob.labels,
                         prob.index_before, prob.mask, prob.field, prob.iterations)
 
+    def set_autotune(self, on: bool = True) -> None:
+        """Times the kernel variants of each fixed length at prepare and keeps the fastest."""
+        check(lib.bwpm_batch_set_autotune(self._h, int(bool(on))))
+
+    def set_variant(self, ny: int, variant: int) -> None:
+        """Forces kernel variant `variant` for length ny (see variant_count)."""
+        check(lib.bwpm_batch_set_variant(self._h, int(ny), int(variant)))
+
+    def classes(self) -> list[dict]:
+        """Kernel classes of the prepared batch: length, threads, CTAs per line, variant."""
+        out = []
+        for k in range(self.stats()["classes"]):
+            v = [ctypes.c_int64() for _ in range(5)]
+            ms = ctypes.c_float()
+            check(lib.bwpm_batch_class_info(self._h, k, *[ctypes.byref(x) for x in v],
+                                            ctypes.byref(ms)))
+            out.append({"ny": v[0].value, "threads": v[1].value, "cluster": v[2].value,
+                        "variant": v[3].value, "items": v[4].value, "tuned_ms": ms.value})
+        return out
+
     def prepare(self) -> None:
         check(lib.bwpm_batch_prepare(self._h))
         self._prepared = True
@@ -110,6 +130,11 @@ class Batch2D:
         check(lib.bwpm_batch_stats(self._h, *[ctypes.byref(x) for x in v]))
         keys = ("device_bytes", "kernel_launches", "work_items", "classes", "packed_inputs")
         return {k: x.value for k, x in zip(keys, v)}
+
+
+def variant_count(ny: int) -> int:
+    """Number of compiled kernel variants for length ny (0: the generic kernels serve it)."""
+    return int(lib.bwpm_variant_count(int(ny)))
 
 
 def flush_l2(device: int = 0, nbytes: int = 512 << 20) -> None:

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <thread>
@@ -22,44 +23,56 @@
 #include "interface.cuh"
 #include "plan.hpp"
 #include "resident2d.cuh"
+#include "variants.hpp"
 
 namespace bwpm {
 namespace {
 
 constexpr int kClassThreads[] = {64, 128, 256, 512};
 constexpr int kGenericClasses = 4;
+constexpr int kMaxFixedLengths = 28;
+constexpr int kNumClasses = kGenericClasses + kMaxFixedLengths;  // ≥ kGenericClasses: fixed length
+constexpr int kTuneSlabs = 48;  // slabs per item in an autotuning run
 
-// Lengths with a compile-time register-resident kernel: N, threads, radices (each divides N/NT).
-struct FixedSpec {
-  int n, nt;
-  std::vector<int> radices;
-};
-const std::vector<FixedSpec>& fixed_specs() {
-  static const std::vector<FixedSpec> specs = {
-      {256, 32, {8, 8, 4}},         {384, 32, {4, 4, 4, 3, 2}},  {512, 32, {16, 8, 4}},
-      {768, 64, {4, 4, 4, 4, 3}},   {1024, 64, {16, 16, 4}},     {1536, 64, {8, 8, 8, 3}},
-      {2048, 128, {16, 16, 8}},     {3072, 128, {8, 8, 8, 3, 2}}, {4096, 256, {16, 16, 16}},
-      {6144, 256, {8, 8, 8, 4, 3}}, {8192, 512, {8, 8, 8, 8, 2}}};
-  return specs;
+// distinct lengths with compiled variants, increasing; class kGenericClasses + i serves entry i
+const std::vector<int>& fixed_lengths() {
+  static const std::vector<int> lengths = [] {
+    std::vector<int> v;
+    for (auto& f : fixed_variants())
+      if (v.empty() || v.back() != f.n) v.push_back(f.n);
+    if (static_cast<int>(v.size()) > kMaxFixedLengths) throw std::logic_error("too many fixed lengths");
+    return v;
+  }();
+  return lengths;
 }
-constexpr int kNumClasses = kGenericClasses + 11;  // class index ≥ kGenericClasses: fixed spec
 
-using rf::Radices;
-// kernel entry of the fixed spec with index `i` (same order as fixed_specs())
-const void* fixed_kernel(int i) {
-  switch (i) {
-    case 0: return (const void*)k_resident2d_fixed<256, 32, Radices<8, 8, 4>>;
-    case 1: return (const void*)k_resident2d_fixed<384, 32, Radices<4, 4, 4, 3, 2>>;
-    case 2: return (const void*)k_resident2d_fixed<512, 32, Radices<16, 8, 4>>;
-    case 3: return (const void*)k_resident2d_fixed<768, 64, Radices<4, 4, 4, 4, 3>>;
-    case 4: return (const void*)k_resident2d_fixed<1024, 64, Radices<16, 16, 4>>;
-    case 5: return (const void*)k_resident2d_fixed<1536, 64, Radices<8, 8, 8, 3>>;
-    case 6: return (const void*)k_resident2d_fixed<2048, 128, Radices<16, 16, 8>>;
-    case 7: return (const void*)k_resident2d_fixed<3072, 128, Radices<8, 8, 8, 3, 2>>;
-    case 8: return (const void*)k_resident2d_fixed<4096, 256, Radices<16, 16, 16>>;
-    case 9: return (const void*)k_resident2d_fixed<6144, 256, Radices<8, 8, 8, 4, 3>>;
-    default: return (const void*)k_resident2d_fixed<8192, 512, Radices<8, 8, 8, 8, 2>>;
+int fixed_length_index(int n) {
+  const auto& l = fixed_lengths();
+  auto it = std::lower_bound(l.begin(), l.end(), n);
+  return it != l.end() && *it == n ? static_cast<int>(it - l.begin()) : -1;
+}
+
+// indices into fixed_variants() of the variants of length n (first: the default)
+std::vector<int> variants_of(int n) {
+  std::vector<int> v;
+  const auto& all = fixed_variants();
+  for (std::size_t i = 0; i < all.size(); ++i)
+    if (all[i].n == n) v.push_back(static_cast<int>(i));
+  return v;
+}
+
+// Autotuning results shared by every batch of the process: (length, log2 of the class's item
+// count) -> variant index.
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, int> g_tuned;
+
+int ilog2(int x) {
+  int r = 0;
+  while (x > 1) {
+    x >>= 1;
+    ++r;
   }
+  return r;
 }
 
 // Operator table job: M/N of `kind` for (ñ_r, ñ_s), entry m00 (E_x) at out[0..2N) and m11 (E_y)
@@ -220,6 +233,30 @@ class Batch2DImpl final : public Batch2D {
 
   void prepare() override;
   void set_graphs(bool on) override { use_graphs_ = on; }
+  void set_autotune(bool on) override { autotune_ = on; }
+  void set_variant(int n, int k) override {
+    if (prepared_) throw invalid_argument("batch already prepared");
+    if (fixed_length_index(n) < 0) throw invalid_argument("ny = " + std::to_string(n) + " has no fixed variants");
+    forced_[n] = k;
+  }
+  int class_info(int k, int& n, int& threads, int& cluster, int& variant, float& tuned_ms) const override {
+    int seen = 0;
+    for (int c = 0; c < kNumClasses; ++c) {
+      if (!class_count_[c]) continue;
+      if (seen++ != k) continue;
+      n = c >= kGenericClasses ? fixed_lengths()[c - kGenericClasses] : class_maxn_[c];
+      threads = class_threads_[c];
+      cluster = c >= kGenericClasses ? fixed_variants()[class_variant_[c]].cluster : 1;
+      variant = -1;
+      if (c >= kGenericClasses) {
+        const std::vector<int> vs = variants_of(n);
+        variant = static_cast<int>(std::find(vs.begin(), vs.end(), class_variant_[c]) - vs.begin());
+      }
+      tuned_ms = class_tuned_ms_[c];
+      return class_count_[c];
+    }
+    throw invalid_argument("no class " + std::to_string(k));
+  }
   void enqueue() override;
   bool ready() override;
   float run() override;
@@ -244,6 +281,8 @@ class Batch2DImpl final : public Batch2D {
   void launch_classes(cudaStream_t origin);
   void capture_graphs();
   void download();
+  void use_variant(int c, int v);
+  void autotune();
   template <typename K, typename... A>
   void launch(K kernel, dim3 grid, dim3 block, std::size_t smem, cudaStream_t s, A... args) {
     kernel<<<grid, block, smem, s>>>(args...);
@@ -269,8 +308,11 @@ class Batch2DImpl final : public Batch2D {
   int class_threads_[kNumClasses] = {};
   std::size_t class_smem_[kNumClasses] = {};
   const void* class_fn_[kNumClasses] = {};
-  std::map<int, int> plan_twbase_, plan_fixed_;
-  bool fixed_enabled_ = true;
+  int class_variant_[kNumClasses] = {};
+  float class_tuned_ms_[kNumClasses] = {};
+  std::map<int, int> variant_twbase_;  // variant index -> twiddle pool offset
+  std::map<int, int> forced_;          // length -> variant position among its variants
+  bool autotune_ = false;
   // device pools
   DevBuf<R2Step> d_steps_;
   DevBuf<R2Pass> d_passes_;
@@ -415,22 +457,28 @@ void Batch2DImpl::prepare() {
     for (auto& e : errs)
       if (e) std::rethrow_exception(e);
   }
-  // plans per distinct length, twiddle pool
+  // plans per distinct length (generic kernels) and twiddles of every variant of the fixed
+  // lengths (autotuning may pick any of them)
   std::map<int, int> plan_of;
   std::vector<FftPlan> plans;
   std::vector<Tw<float>> tw;
+  std::map<int, bool> seen_n;
   for (auto& h : solves_) {
     const int n = h.in.ny;
-    if (plan_of.count(n)) continue;
-    int fixed = -1;
-    for (std::size_t f = 0; f < fixed_specs().size(); ++f)
-      if (fixed_specs()[f].n == n && fixed_enabled_) fixed = static_cast<int>(f);
-    HostPlan hp = fixed >= 0 ? make_plan_radices(n, fixed_specs()[fixed].radices) : make_plan(n);
+    if (seen_n.count(n)) continue;
+    seen_n[n] = true;
+    if (fixed_length_index(n) >= 0) {
+      for (int v : variants_of(n)) {
+        const HostPlan hp = make_plan_radices(n, fixed_variants()[v].radices);
+        variant_twbase_[v] = static_cast<int>(tw.size());
+        for (auto& t : twiddles_for<float>(hp)) tw.push_back(t);
+      }
+      continue;
+    }
+    HostPlan hp = make_plan(n);
     const int base = static_cast<int>(tw.size());
-    plan_twbase_[n] = base;
-    plan_fixed_[n] = fixed;
     for (auto& t : twiddles_for<float>(hp)) tw.push_back(t);
-    for (int s = 0; s < hp.plan.nstages; ++s) hp.plan.twoff[s] += base;
+    for (int st = 0; st < hp.plan.nstages; ++st) hp.plan.twoff[st] += base;
     hp.plan.rootoff += base;
     plan_of[n] = static_cast<int>(plans.size());
     plans.push_back(hp.plan);
@@ -462,8 +510,8 @@ void Batch2DImpl::prepare() {
       for (int q = 0; q < n && !any; ++q) any = h.in.field[2 * q + c].re != 0.0 || h.in.field[2 * q + c].im != 0.0;
       if (!any) continue;
       int cls = 0;
-      if (plan_fixed_[n] >= 0) {
-        cls = kGenericClasses + plan_fixed_[n];
+      if (fixed_length_index(n) >= 0) {
+        cls = kGenericClasses + fixed_length_index(n);
       } else {
         const int want = threads_needed(plans[plan_of[n]], 1, kR2Ept);
         if (want > kClassThreads[kGenericClasses - 1])
@@ -625,7 +673,7 @@ void Batch2DImpl::prepare() {
     r.n = n;
     r.nz = h.in.nz;
     r.iterations = h.in.iterations;
-    r.plan = plan_of[n];
+    r.plan = plan_of.count(n) ? plan_of[n] : 0;  // fixed kernels carry their plan
     h_items_[k] = r;
     io[k] = {h.packed, const_cast<cf*>(r.input), r.transmitted, r.reflected, n, itm.comp};
   }
@@ -670,20 +718,28 @@ void Batch2DImpl::prepare() {
   set_attr((const void*)k_resident2d<512>);
   for (int c = 0; c < kNumClasses; ++c) {
     if (!class_count_[c]) continue;
-    const void* k;
-    int threads;
     if (c >= kGenericClasses) {
-      const FixedSpec& f = fixed_specs()[c - kGenericClasses];
-      k = fixed_kernel(c - kGenericClasses);
-      threads = f.nt;
-      class_smem_[c] = 3 * static_cast<std::size_t>(rf::padded(f.n)) * sizeof(cf);
-      set_attr(k);
-    } else {
-      k = c == 0 ? (const void*)k_resident2d<64> : c == 1 ? (const void*)k_resident2d<128>
-          : c == 2 ? (const void*)k_resident2d<256> : (const void*)k_resident2d<512>;
-      threads = kClassThreads[c];
-      class_smem_[c] = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+      const int n = fixed_lengths()[c - kGenericClasses];
+      const std::vector<int> vs = variants_of(n);
+      for (int v : vs) set_attr(fixed_variants()[v].fn);
+      int pick = vs.front();
+      auto f = forced_.find(n);
+      if (f != forced_.end()) {
+        if (f->second < 0 || f->second >= static_cast<int>(vs.size()))
+          throw invalid_argument("no variant " + std::to_string(f->second) + " for ny = " + std::to_string(n));
+        pick = vs[f->second];
+      } else {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto t = g_tuned.find({n, ilog2(class_count_[c])});
+        if (t != g_tuned.end()) pick = t->second;
+      }
+      use_variant(c, pick);
+      continue;
     }
+    const void* k = c == 0 ? (const void*)k_resident2d<64> : c == 1 ? (const void*)k_resident2d<128>
+                    : c == 2 ? (const void*)k_resident2d<256> : (const void*)k_resident2d<512>;
+    const int threads = kClassThreads[c];
+    class_smem_[c] = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
     int per_sm = 0;
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, class_smem_[c]), "occupancy");
     per_sm = std::max(1, per_sm);
@@ -691,6 +747,7 @@ void Batch2DImpl::prepare() {
     class_threads_[c] = threads;
     class_fn_[c] = k;
   }
+  if (autotune_) autotune();
   bytes_ = d_steps_.bytes() + d_passes_.bytes() + d_pids_.bytes() + d_iface_.bytes() +
            d_tables_.bytes() + d_twiddles_.bytes() + d_lines_.bytes() + d_src_.bytes() +
            d_mask_.bytes() + d_weights_.bytes() + d_energy_.bytes() + d_packed_in_.bytes() +
@@ -723,8 +780,7 @@ void Batch2DImpl::launch_classes(cudaStream_t origin) {
     int* q = d_queue_.ptr + c;
     const dim3 grid(class_grid_[c]), block(class_threads_[c]);
     if (c >= kGenericClasses) {
-      const int n = fixed_specs()[c - kGenericClasses].n;
-      const Tw<float>* tw = d_twiddles_.ptr + plan_twbase_[n];
+      const Tw<float>* tw = d_twiddles_.ptr + variant_twbase_[class_variant_[c]];
       void* args[] = {&items, &count, &q, &tw};
       check_cuda(cudaLaunchKernel(class_fn_[c], grid, block, args, class_smem_[c], s), "launch");
     } else {
@@ -736,6 +792,77 @@ void Batch2DImpl::launch_classes(cudaStream_t origin) {
     check_cuda(cudaEventRecord(class_done_[c], s), "event");
     check_cuda(cudaStreamWaitEvent(origin, class_done_[c], 0), "wait");
   }
+}
+
+void Batch2DImpl::use_variant(int c, int v) {
+  const FixedVariant& f = fixed_variants()[v];
+  int per_sm = 0;
+  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f.fn, f.nt, f.smem), "occupancy");
+  per_sm = std::max(1, per_sm);
+  class_variant_[c] = v;
+  class_fn_[c] = f.fn;
+  class_threads_[c] = f.nt;
+  class_smem_[c] = f.smem;
+  class_grid_[c] = std::min(class_count_[c], per_sm * sms_);
+}
+
+// Times every variant of each fixed-length class on the class's own items, chains cut to
+// kTuneSlabs slabs and at most one iteration, and keeps the fastest (shared by later batches of
+// the process with the same length and item-count bucket). The cut runs write only into this
+// batch's own output and source buffers, which every full run rewrites before reading.
+void Batch2DImpl::autotune() {
+  cudaEvent_t a, b;
+  check_cuda(cudaEventCreate(&a), "event");
+  check_cuda(cudaEventCreate(&b), "event");
+  for (int c = kGenericClasses; c < kNumClasses; ++c) {
+    if (!class_count_[c]) continue;
+    const int n = fixed_lengths()[c - kGenericClasses];
+    const std::vector<int> vs = variants_of(n);
+    if (vs.size() < 2 || forced_.count(n)) continue;
+    const std::pair<int, int> key{n, ilog2(class_count_[c])};
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      if (g_tuned.count(key)) continue;
+    }
+    std::vector<R2Item> cut(h_items_.begin() + class_first_[c], h_items_.begin() + class_first_[c] + class_count_[c]);
+    for (auto& it : cut) {
+      it.nz = std::min(it.nz, kTuneSlabs);
+      it.iterations = std::min(it.iterations, 1);
+    }
+    DevBuf<R2Item> d_cut(cut.size(), main_.s);
+    d_cut.upload(cut.data(), cut.size());
+    float best = 1e30f;
+    int best_v = vs.front();
+    for (int v : vs) {
+      use_variant(c, v);
+      const R2Item* items = d_cut.ptr;
+      int count = class_count_[c];
+      int* q = d_queue_.ptr + c;
+      const Tw<float>* tw = d_twiddles_.ptr + variant_twbase_[v];
+      void* args[] = {&items, &count, &q, &tw};
+      float ms = 0;
+      for (int rep = 0; rep < 2; ++rep) {  // the first run warms caches and the instruction cache
+        check_cuda(cudaMemsetAsync(q, 0, sizeof(int), main_), "queue reset");
+        check_cuda(cudaEventRecord(a, main_), "event");
+        check_cuda(cudaLaunchKernel(class_fn_[c], dim3(class_grid_[c]), dim3(class_threads_[c]), args,
+                                    class_smem_[c], main_), "launch");
+        check_cuda(cudaEventRecord(b, main_), "event");
+        check_cuda(cudaEventSynchronize(b), "autotune");
+        check_cuda(cudaEventElapsedTime(&ms, a, b), "elapsed");
+        launches_ += 1;
+      }
+      if (ms < best) {
+        best = ms;
+        best_v = v;
+      }
+    }
+    use_variant(c, best_v);
+    class_tuned_ms_[c] = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best_v;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
 }
 
 void Batch2DImpl::capture_graphs() {

@@ -44,6 +44,15 @@ class Batch2D {
   virtual void prepare() = 0;
   // off: no CUDA graphs are captured at prepare (single-use batches); default on
   virtual void set_graphs(bool on) = 0;
+  // on: prepare() times the kernel variants of each fixed length on the batch's own items
+  // (chains cut short) and keeps the fastest; results are cached for the process. Default off
+  // (the first listed variant, or a cached choice).
+  virtual void set_autotune(bool on) = 0;
+  // forces variant k (position among the variants of length n) for this batch
+  virtual void set_variant(int n, int k) = 0;
+  // class k (0 ≤ k < classes()): length (the largest for a generic class), threads, CTAs per
+  // line, variant position (−1: generic kernel), autotuned ms (0: not tuned); returns its items
+  virtual int class_info(int k, int& n, int& threads, int& cluster, int& variant, float& tuned_ms) const = 0;
   // enqueues one batched solve on the batch's stream and returns at once; ready() tells whether
   // it has finished (results then come from result())
   virtual void enqueue() = 0;

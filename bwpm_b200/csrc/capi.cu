@@ -9,6 +9,7 @@
 #include "noalloc.hpp"
 #include "server.hpp"
 #include "solver.hpp"
+#include "variants.hpp"
 
 struct bwpm_solver {
   std::unique_ptr<bwpm::Solver> impl;
@@ -172,6 +173,42 @@ int bwpm_batch_add(bwpm_batch* b, size_t ny, double dy, double dz, double k0,
     const int64_t k = b->impl->add(std::move(s));
     if (id) *id = k;
   });
+}
+
+int bwpm_batch_set_autotune(bwpm_batch* b, int on) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    b->impl->set_autotune(on != 0);
+  });
+}
+
+int bwpm_batch_set_variant(bwpm_batch* b, size_t ny, int variant) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    b->impl->set_variant(static_cast<int>(ny), variant);
+  });
+}
+
+int bwpm_batch_class_info(const bwpm_batch* b, int64_t k, int64_t* ny, int64_t* threads,
+                          int64_t* cluster, int64_t* variant, int64_t* items, float* tuned_ms) {
+  return guarded([&] {
+    if (!b || !b->impl) throw bwpm::invalid_argument("null batch");
+    int n = 0, t = 0, c = 0, v = 0;
+    float ms = 0;
+    const int count = b->impl->class_info(static_cast<int>(k), n, t, c, v, ms);
+    if (ny) *ny = n;
+    if (threads) *threads = t;
+    if (cluster) *cluster = c;
+    if (variant) *variant = v;
+    if (items) *items = count;
+    if (tuned_ms) *tuned_ms = ms;
+  });
+}
+
+int bwpm_variant_count(size_t ny) {
+  int k = 0;
+  for (const auto& v : bwpm::fixed_variants()) k += v.n == static_cast<int>(ny);
+  return k;
 }
 
 int bwpm_batch_prepare(bwpm_batch* b) {

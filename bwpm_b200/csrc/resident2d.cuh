@@ -65,7 +65,7 @@ __device__ __forceinline__ long long global_ns() {
 }
 
 // Σ w[q]·|buf[q]|² over the line, FP64 with compensated block reduction; thread 0 returns it.
-__device__ double r2_flux(const cf* buf, const double* w, int n, double* red) {
+__device__ inline double r2_flux(const cf* buf, const double* w, int n, double* red) {
   double s = 0.0, c = 0.0;
   for (int q = threadIdx.x; q < n; q += blockDim.x) {
     const double v = w[q] * (static_cast<double>(buf[q].re) * buf[q].re +

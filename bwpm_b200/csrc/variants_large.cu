@@ -1,0 +1,28 @@
+// Kernel variants of the resident 2D engine for lengths 2048-8192 (see variants.hpp).
+#include "resident2d.cuh"
+#include "variants.hpp"
+
+namespace bwpm {
+
+namespace {
+using rf::Radices;
+
+template <int N, int NT, int... R>
+FixedVariant fixed() {
+  return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>,
+          3 * static_cast<std::size_t>(rf::padded(N)) * sizeof(cf)};
+}
+}  // namespace
+
+void add_variants_large(std::vector<FixedVariant>& v) {
+  v.push_back(fixed<2048, 128, 16, 16, 8>());
+  v.push_back(fixed<2048, 256, 8, 8, 8, 4>());
+  v.push_back(fixed<3072, 256, 4, 4, 4, 4, 4, 3>());
+  v.push_back(fixed<3072, 128, 8, 8, 8, 3, 2>());
+  v.push_back(fixed<4096, 256, 16, 16, 16>());
+  v.push_back(fixed<6144, 256, 8, 8, 8, 4, 3>());
+  v.push_back(fixed<6144, 512, 4, 4, 4, 4, 4, 2, 3>());
+  v.push_back(fixed<8192, 512, 8, 8, 8, 8, 2>());
+}
+
+}  // namespace bwpm

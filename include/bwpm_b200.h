@@ -92,6 +92,22 @@ int bwpm_batch_add(bwpm_batch* b, size_t ny, double dy, double dz, double k0,
                    double index_before_re, double index_before_im, const double* mask,
                    const double* field, int iterations, int64_t* id);
 
+/* Kernel choice per line length (before prepare). Lengths with compiled register-resident
+ * kernels (bwpm_variant_count(ny) > 0) have one or more variants (threads per CTA, FFT radices,
+ * CTAs per line). on = 1: prepare times every variant of each such length on the batch's own
+ * items (chains cut short) and keeps the fastest; choices are kept for the process. Default:
+ * the first variant, or a choice made earlier in the process. set_variant forces variant
+ * `variant` (0-based) for length ny. */
+int bwpm_batch_set_autotune(bwpm_batch* b, int on);
+int bwpm_batch_set_variant(bwpm_batch* b, size_t ny, int variant);
+int bwpm_variant_count(size_t ny);
+
+/* Class k of a prepared batch (k < classes of bwpm_batch_stats): line length (the largest of a
+ * generic class), threads per CTA, CTAs per line, variant (−1: generic kernel), work items and
+ * the autotuned time of the chosen variant in ms (0: not tuned). */
+int bwpm_batch_class_info(const bwpm_batch* b, int64_t k, int64_t* ny, int64_t* threads,
+                          int64_t* cluster, int64_t* variant, int64_t* items, float* tuned_ms);
+
 /* Builds the device pools, operator tables and launch shapes (once, after the last add). */
 int bwpm_batch_prepare(bwpm_batch* b);
 

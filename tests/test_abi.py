@@ -43,3 +43,13 @@ def test_errors_map_to_value_error():
 
     with pytest.raises(ValueError, match="labels must have shape"):
         _core.CudaSolver(4, 1, 1.0, 1.0, 1.0, 1.0, np.array([1.0]), np.zeros((2, 4)), 1.0, None)
+
+
+def test_every_batched_length_has_a_kernel_variant():
+    """The lengths of the batched workload all have compiled register-resident kernels."""
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import variant_count
+
+    for n in workloads.BATCH_SIZES:
+        assert variant_count(n) >= 1, n
+    assert variant_count(1000) == 0  # served by the generic kernels

@@ -150,3 +150,56 @@ def test_solve_packed_round_trip():
         assert np.array_equal(out[off:off + n2].reshape(p.ny, 2), r["transmitted"])
         assert np.array_equal(out[off + n2:off + 2 * n2].reshape(p.ny, 2), r["reflected"])
         off += 2 * n2
+
+
+FIXED_LENGTHS = (256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096, 6144, 8192)
+
+
+def _variant_problem(n):
+    from bwpm_b200 import workloads
+
+    prm = dict(i=n, ny=n, nz=40, wl=0.55, theta=0.2, n=1.6, tilt=0.1, iterations=2)
+    return workloads.tilted_slab2d_from(prm)
+
+
+@pytest.mark.parametrize("n", FIXED_LENGTHS)
+def test_every_kernel_variant_matches_fp64(n):
+    """Each compiled kernel variant of a length (threads, radices, CTAs per line) against FP64."""
+    from bwpm_b200.batch import Batch2D, variant_count
+
+    p = _variant_problem(n)
+    ref = _fp64(p)
+    count = variant_count(n)
+    assert count >= 1
+    for k in range(count):
+        b = Batch2D()
+        b.set_variant(n, k)
+        i = b.add_problem(p)
+        b.run()
+        cls = b.classes()
+        assert cls[0]["variant"] == k and cls[0]["ny"] == n
+        r = b.result(i)
+        assert rel_l2(r["transmitted"], ref["transmitted"][:, 0]) < L2_C64, (n, k, cls[0])
+        assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64, (n, k, cls[0])
+
+
+def test_autotuned_batch_equals_forced_variant():
+    """Autotuning picks a variant per length; the results equal a run forced to that variant."""
+    from bwpm_b200 import workloads
+    from bwpm_b200.batch import Batch2D
+
+    probs = workloads.batch2d(count=8, seed=31, sizes=(512, 1536, 3072), nz_range=(30, 60),
+                              iterations=2)
+    b = Batch2D()
+    b.set_autotune(True)
+    ids = [b.add_problem(p) for p in probs]
+    b.run()
+    cls = {c["ny"]: c for c in b.classes()}
+    assert all(c["tuned_ms"] > 0 for c in cls.values())
+    forced = Batch2D()
+    for n, c in cls.items():
+        forced.set_variant(n, c["variant"])
+    fids = [forced.add_problem(p) for p in probs]
+    forced.run()
+    for i, j in zip(ids, fids):
+        assert np.array_equal(b.result(i)["transmitted"], forced.result(j)["transmitted"])
