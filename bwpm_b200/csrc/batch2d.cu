@@ -66,6 +66,26 @@ std::vector<int> variants_of(int n) {
 std::mutex g_tune_mu;
 std::map<std::pair<int, int>, int> g_tuned;
 
+// Twiddles of a variant: the stage twiddles of its per-CTA transform (N/C points); for a line
+// split over C CTAs followed by the cross twiddles w_N^{c·k1} (c < C, k1 < N/C), all (hi, lo).
+std::vector<Tw<float>> variant_twiddles(const FixedVariant& f) {
+  const int m = f.n / f.cluster;
+  const HostPlan hp = make_plan_radices(m, f.radices);
+  std::vector<Tw<float>> t = twiddles_for<float>(hp);
+  if (f.cluster == 1) return t;
+  t.resize(static_cast<std::size_t>(hp.plan.rootoff));  // the M − 1 stage twiddles
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int c = 0; c < f.cluster; ++c)
+    for (int k = 0; k < m; ++k) {
+      const long long e = (static_cast<long long>(c) * k) % f.n;
+      const double a = -two_pi * static_cast<double>(e) / static_cast<double>(f.n);
+      const cd w{std::cos(a), std::sin(a)};
+      const cf h{static_cast<float>(w.re), static_cast<float>(w.im)};
+      t.push_back(Tw<float>{h, cf{static_cast<float>(w.re - h.re), static_cast<float>(w.im - h.im)}});
+    }
+  return t;
+}
+
 int ilog2(int x) {
   int r = 0;
   while (x > 1) {
@@ -469,9 +489,8 @@ void Batch2DImpl::prepare() {
     seen_n[n] = true;
     if (fixed_length_index(n) >= 0) {
       for (int v : variants_of(n)) {
-        const HostPlan hp = make_plan_radices(n, fixed_variants()[v].radices);
         variant_twbase_[v] = static_cast<int>(tw.size());
-        for (auto& t : twiddles_for<float>(hp)) tw.push_back(t);
+        for (auto& t : variant_twiddles(fixed_variants()[v])) tw.push_back(t);
       }
       continue;
     }
@@ -796,14 +815,24 @@ void Batch2DImpl::launch_classes(cudaStream_t origin) {
 
 void Batch2DImpl::use_variant(int c, int v) {
   const FixedVariant& f = fixed_variants()[v];
-  int per_sm = 0;
-  check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f.fn, f.nt, f.smem), "occupancy");
-  per_sm = std::max(1, per_sm);
   class_variant_[c] = v;
   class_fn_[c] = f.fn;
   class_threads_[c] = f.nt;
   class_smem_[c] = f.smem;
-  class_grid_[c] = std::min(class_count_[c], per_sm * sms_);
+  if (f.cluster == 1) {
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f.fn, f.nt, f.smem), "occupancy");
+    class_grid_[c] = std::min(class_count_[c], std::max(1, per_sm) * sms_);
+    return;
+  }
+  // clusters of f.cluster CTAs (compile-time cluster size of the kernel)
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(static_cast<unsigned>(f.cluster * sms_));
+  cfg.blockDim = dim3(static_cast<unsigned>(f.nt));
+  cfg.dynamicSmemBytes = f.smem;
+  int clusters = 0;
+  check_cuda(cudaOccupancyMaxActiveClusters(&clusters, f.fn, &cfg), "cluster occupancy");
+  class_grid_[c] = std::min(class_count_[c], std::max(1, clusters)) * f.cluster;
 }
 
 // Times every variant of each fixed-length class on the class's own items, chains cut to

@@ -1,0 +1,315 @@
+// Resident 2D engine, one line split over a cluster of C CTAs (thread-block cluster + DSMEM).
+//
+// For the longest lines one CTA per line makes the slab chain latency-bound (one SM's issue
+// rate and register file). Here the C CTAs of a cluster, on C SMs, share one work item:
+// N = C·M, CTA c holds the real-space points n = C·m + c (m < M) and the spectral points
+// k = c·(M/C) + k1l + M·k2 (k1l < M/C, k2 < C). A length-N transform is
+//   forward:  Y_c = DFT_M(x_c);  Y_c[k1] ·= w_N^{c·k1};  exchange;
+//             X[k1 + M·k2] = Σ_c Y_c[k1]·w_C^{c·k2}   (C-point DFT over the cluster)
+//   inverse:  Z_c[k1] = Σ_k2 X[k1 + M·k2]·w_C^{−c·k2}·w_N^{−c·k1};  exchange;
+//             x_c = IDFT_M(Z_c)
+// (a two-factor Cooley-Tukey split, N = M·C), each exchange one all-to-all through distributed
+// shared memory between two cluster barriers' worth of work. The local M-point transforms are
+// the register-resident transforms of rfft.cuh. Exchange buffers alternate, so one cluster
+// barrier per exchange suffices: a buffer is written again only after a later exchange's
+// barrier, which every CTA reaches after its reads of the earlier one.
+//
+// Everything else (passes, selection by pair id, mask, interface sources, FP64 flux) follows
+// k_resident2d_fixed; each CTA handles its own points. Cross twiddles w_N^{c·k1} (c < C,
+// k1 < M) are (hi, lo) pairs from FP64, stored after the M-point plan's twiddles (which hold
+// M − 1 entries for any radix order).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "resident2d.cuh"
+
+namespace bwpm {
+namespace r2c {
+
+namespace cg = cooperative_groups;
+
+template <int N, int C, int NT>
+struct Shape {
+  static constexpr int M = N / C;      // points per CTA
+  static constexpr int E = M / NT;     // values per thread
+  static constexpr int EB = E / C;     // spectral slots per thread and k2
+  static constexpr int MB = M / C;     // spectral k1 block of one CTA
+  static_assert(N % C == 0 && M % NT == 0 && E % C == 0, "cluster shape");
+};
+
+// spectral index of slot s (= k2·EB + i) of thread t in CTA c
+template <int N, int C, int NT>
+__device__ __forceinline__ int kspec(int s, int t, int c) {
+  using S = Shape<N, C, NT>;
+  const int k2 = s / S::EB, i = s % S::EB;
+  return c * S::MB + i * NT + t + S::M * k2;
+}
+
+// real-space index of owned value j of thread t in CTA c
+template <int N, int C, int NT>
+__device__ __forceinline__ int qreal(int j, int t, int c) {
+  return C * (t + j * NT) + c;
+}
+
+// Forward N-point transform: v holds the CTA's real-space values (owned pattern of the M-point
+// transform) and receives its spectral slots.
+template <int N, int C, int NT, class RADS>
+__device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
+                                        cf* const (&xb)[2], int& xphase, const Tw<float>* tw,
+                                        const Tw<float>* xtw, int t, int c, cg::cluster_group& cl) {
+  using S = Shape<N, C, NT>;
+  rf::fft<-1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
+  cf* x = xb[xphase];
+#pragma unroll
+  for (int j = 0; j < S::E; ++j) {
+    const int k1 = t + j * NT;
+    x[k1] = c == 0 ? v[j] : twmul<-1>(v[j], xtw[c * S::M + k1]);
+  }
+  cl.sync();
+#pragma unroll
+  for (int i = 0; i < S::EB; ++i) {
+    const int k1 = c * S::MB + i * NT + t;
+    cf u[C];
+#pragma unroll
+    for (int r = 0; r < C; ++r) u[r] = cl.map_shared_rank(x, r)[k1];
+    rf::dft<-1, C>(u);
+#pragma unroll
+    for (int k2 = 0; k2 < C; ++k2) v[k2 * S::EB + i] = u[k2];
+  }
+  xphase ^= 1;
+}
+
+// Inverse (unnormalised) N-point transform: spectral slots in, real-space owned values out.
+template <int N, int C, int NT, class RADS>
+__device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
+                                        cf* const (&xb)[2], int& xphase, const Tw<float>* tw,
+                                        const Tw<float>* xtw, int t, int c, cg::cluster_group& cl) {
+  using S = Shape<N, C, NT>;
+  cf* x = xb[xphase];
+#pragma unroll
+  for (int i = 0; i < S::EB; ++i) {
+    const int k1l = i * NT + t, k1 = c * S::MB + k1l;
+    cf u[C];
+#pragma unroll
+    for (int k2 = 0; k2 < C; ++k2) u[k2] = v[k2 * S::EB + i];
+    rf::dft<+1, C>(u);
+#pragma unroll
+    for (int d = 0; d < C; ++d) x[d * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xtw[d * S::M + k1]);
+  }
+  cl.sync();
+#pragma unroll
+  for (int j = 0; j < S::E; ++j) {
+    // k1 = t + j·NT lies in the block of CTA j / EB, at local index (j mod EB)·NT + t
+    const cf* src = cl.map_shared_rank(x, j / S::EB);
+    v[j] = src[c * S::MB + (j % S::EB) * NT + t];
+  }
+  xphase ^= 1;
+  rf::fft<+1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
+}
+
+// Σ w[k]·|v|² over the CTA's spectral slots, compensated FP64; the cluster total is returned on
+// rank 0 (others return 0). `part` is this CTA's shared slot for its partial sum.
+template <int N, int C, int NT>
+__device__ __forceinline__ double flux(const cf (&v)[Shape<N, C, NT>::E], const double* w,
+                                       double* red, double* part, int t, int c,
+                                       cg::cluster_group& cl) {
+  using S = Shape<N, C, NT>;
+  double s = 0.0, comp = 0.0;
+#pragma unroll
+  for (int j = 0; j < S::E; ++j) {
+    const double a = w[kspec<N, C, NT>(j, t, c)] * (static_cast<double>(v[j].re) * v[j].re +
+                                                     static_cast<double>(v[j].im) * v[j].im);
+    const double y = a - comp;
+    const double z = s + y;
+    comp = (z - s) - y;
+    s = z;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((t & 31) == 0) red[t >> 5] = s;
+  __syncthreads();
+  if (t == 0) {
+    double total = 0.0, cc = 0.0;
+    for (int i = 0; i < NT / 32; ++i) {
+      const double y = red[i] - cc;
+      const double z = total + y;
+      cc = (z - total) - y;
+      total = z;
+    }
+    *part = total;
+  }
+  cl.sync();
+  double total = 0.0;
+  if (c == 0 && t == 0) {
+    double cc = 0.0;
+    for (int r = 0; r < C; ++r) {
+      const double y = *cl.map_shared_rank(part, r) - cc;
+      const double z = total + y;
+      cc = (z - total) - y;
+      total = z;
+    }
+  }
+  // the partials are rewritten at the next flux, after at least one more cluster barrier
+  return total;
+}
+
+// One slab step of the CTA's share of an item (cf. r2f_step).
+template <int N, int C, int NT, class RADS>
+__device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&out)[Shape<N, C, NT>::E],
+                                     cf* b0, cf* b1, int& phase, cf* const (&xb)[2], int& xphase,
+                                     const R2Item& it, const R2Step& st, bool backward, bool reflect,
+                                     cf* store, const cf* add, const Tw<float>* tw,
+                                     const Tw<float>* xtw, int t, int c, cg::cluster_group& cl) {
+  using Sh = Shape<N, C, NT>;
+  constexpr int E = Sh::E;
+  const int off = backward ? st.bwd_off : st.fwd_off;
+  const int ntp = backward ? st.bwd_t : st.fwd_t;
+  const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
+  const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
+  const int* iface = it.iface + st.iface;
+  forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+  if (npass == 1) {
+    const cf* m = it.tables + it.passes[off].tab;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int k = kspec<N, C, NT>(j, t, c);
+      v[j] = pmul(v[j], m[k], m[N + k]);
+    }
+    inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+    if (it.mask)
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int q = qreal<N, C, NT>(j, t, c);
+        v[j] = mask_mul(v[j], it.mask[q], it.mask[N + q]);
+      }
+  } else {
+#pragma unroll
+    for (int j = 0; j < E; ++j) S[rf::pad(t + j * NT)] = v[j];
+    for (int p = 0; p < npass; ++p) {
+      const R2Pass ps = it.passes[off + p];
+      const cf* m = it.tables + ps.tab;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int k = kspec<N, C, NT>(j, t, c);
+        v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
+      }
+      inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+      if (!ps.refl) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+          const int q = qreal<N, C, NT>(j, t, c);
+          if (!pid || pid[q] == ps.pair) out[j] = it.mask ? mask_mul(v[j], it.mask[q], it.mask[N + q]) : v[j];
+        }
+      } else {  // gather at this CTA's interface pixels through the free exchange buffer
+        cf* buf = phase ? b1 : b0;
+#pragma unroll
+        for (int j = 0; j < E; ++j) buf[rf::pad(t + j * NT)] = v[j];
+        __syncthreads();
+        for (int k = t; k < st.niface; k += NT) {
+          const int q = iface[k];
+          if (q % C != c) continue;
+          if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q / C)];
+        }
+        phase ^= 1;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = out[j];
+  }
+  if (add) {  // sparse sources of the other pass at this CTA's interface pixels
+    cf* buf = phase ? b1 : b0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) buf[rf::pad(t + j * NT)] = v[j];
+    __syncthreads();
+    for (int k = t; k < st.niface; k += NT) {
+      const int q = iface[k];
+      if (q % C != c) continue;
+      const int m = rf::pad(q / C);
+      buf[m] = buf[m] + add[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = buf[rf::pad(t + j * NT)];
+    phase ^= 1;
+  }
+}
+
+}  // namespace r2c
+
+// Persistent cluster kernel: each cluster pulls work items from `queue` (rank 0 takes the next
+// index and shares it through distributed shared memory).
+template <int N, int C, int NT, class RADS>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
+    k_resident2d_cluster(const R2Item* __restrict__ items, int nitems, int* queue,
+                         const Tw<float>* __restrict__ tw) {
+  using S = r2c::Shape<N, C, NT>;
+  constexpr int E = S::E;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cf* b0 = reinterpret_cast<cf*>(smem_raw);
+  cf* b1 = b0 + rf::padded(S::M);
+  cf* Sl = b1 + rf::padded(S::M);
+  cf* const xb[2] = {Sl + rf::padded(S::M), Sl + rf::padded(S::M) + S::M};
+  __shared__ int s_item;
+  __shared__ double s_red[NT / 32];
+  __shared__ double s_part;
+  r2c::cg::cluster_group cl = r2c::cg::this_cluster();
+  const int t = threadIdx.x;
+  const int c = static_cast<int>(cl.block_rank());
+  const Tw<float>* xtw = tw + (S::M - 1);
+  int phase = 0, xphase = 0;
+  for (;;) {
+    if (c == 0 && t == 0) s_item = atomicAdd(queue, 1);
+    cl.sync();
+    const int idx = *cl.map_shared_rank(&s_item, 0);
+    if (idx >= nitems) {  // every CTA of the cluster leaves together, after every CTA has read
+      cl.sync();          // rank 0's index (no CTA exits while a peer reads its shared memory)
+      return;
+    }
+    const R2Item it = items[idx];
+    if (c == 0 && t == 0) it.clock[0] = global_ns();
+    cf v[E], out[E];
+    const int iters = it.iterations > 0 ? it.iterations : 1;
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = it.input[r2c::qreal<N, C, NT>(j, t, c)];
+    r2c::forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+    {
+      const double pin = r2c::flux<N, C, NT>(v, it.w_in, s_red, &s_part, t, c, cl);
+      if (c == 0 && t == 0) it.energy[2 * iters] = pin;
+    }
+    const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
+    for (int sw = 0; sw < sweeps; ++sw) {
+      const bool backward = sw & 1;
+      const int iter = sw >> 1;
+      if (!backward) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[j] = it.input[r2c::qreal<N, C, NT>(j, t, c)];
+      } else {
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[j] = cf{0.f, 0.f};
+      }
+      for (int s = 0; s < it.nz; ++s) {
+        const int p = backward ? it.nz - 1 - s : s;
+        const R2Step st = it.steps[p];
+        const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
+        const bool has_add = st.niface > 0 && (backward || iter > 0);
+        cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
+        const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
+        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, xb, xphase, it, st, backward, reflect,
+                                  store, add, tw, xtw, t, c, cl);
+      }
+      cf* dst = backward ? it.reflected : it.transmitted;
+#pragma unroll
+      for (int j = 0; j < E; ++j) dst[r2c::qreal<N, C, NT>(j, t, c)] = v[j];
+      if (it.iterations == 0) break;
+#pragma unroll
+      for (int j = 0; j < E; ++j) out[j] = v[j];
+      r2c::forward<N, C, NT, RADS>(out, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+      const double fl = r2c::flux<N, C, NT>(out, backward ? it.w_in : it.w_out, s_red, &s_part, t, c, cl);
+      if (c == 0 && t == 0) it.energy[2 * iter + (backward ? 1 : 0)] = fl;
+    }
+    cl.sync();  // the whole cluster is done with the item
+    if (c == 0 && t == 0) it.clock[1] = global_ns();
+  }
+}
+
+}  // namespace bwpm

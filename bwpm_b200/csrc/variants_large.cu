@@ -1,4 +1,5 @@
 // Kernel variants of the resident 2D engine for lengths 2048-8192 (see variants.hpp).
+#include "cluster2d.cuh"
 #include "resident2d.cuh"
 #include "variants.hpp"
 
@@ -12,17 +13,32 @@ FixedVariant fixed() {
   return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>,
           3 * static_cast<std::size_t>(rf::padded(N)) * sizeof(cf)};
 }
+// one line over a cluster of C CTAs: 3 transform lines of M = N/C points + 2 exchange buffers
+template <int N, int C, int NT, int... R>
+FixedVariant cluster() {
+  constexpr int M = N / C;
+  return {N, NT, C, {R...}, (const void*)k_resident2d_cluster<N, C, NT, Radices<R...>>,
+          (3 * static_cast<std::size_t>(rf::padded(M)) + 2 * static_cast<std::size_t>(M)) * sizeof(cf)};
+}
 }  // namespace
 
 void add_variants_large(std::vector<FixedVariant>& v) {
-  v.push_back(fixed<2048, 128, 16, 16, 8>());
   v.push_back(fixed<2048, 256, 8, 8, 8, 4>());
+  v.push_back(fixed<2048, 128, 16, 16, 8>());
+  v.push_back(cluster<2048, 2, 128, 8, 8, 8, 2>());
   v.push_back(fixed<3072, 256, 4, 4, 4, 4, 4, 3>());
   v.push_back(fixed<3072, 128, 8, 8, 8, 3, 2>());
+  v.push_back(cluster<3072, 2, 128, 4, 4, 4, 4, 2, 3>());
   v.push_back(fixed<4096, 256, 16, 16, 16>());
+  v.push_back(cluster<4096, 2, 256, 8, 8, 8, 4>());
+  v.push_back(cluster<4096, 4, 128, 8, 8, 8, 2>());
   v.push_back(fixed<6144, 256, 8, 8, 8, 4, 3>());
   v.push_back(fixed<6144, 512, 4, 4, 4, 4, 4, 2, 3>());
+  v.push_back(cluster<6144, 2, 256, 4, 4, 4, 4, 4, 3>());
+  v.push_back(cluster<6144, 4, 128, 4, 4, 4, 4, 2, 3>());
   v.push_back(fixed<8192, 512, 8, 8, 8, 8, 2>());
+  v.push_back(cluster<8192, 2, 512, 8, 8, 8, 8>());
+  v.push_back(cluster<8192, 4, 256, 8, 8, 8, 4>());
 }
 
 }  // namespace bwpm
