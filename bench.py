@@ -304,6 +304,7 @@ def run_ours(args) -> None:
     kern_s = step_ms * 1e-3
     achieved = work["flops"] / kern_s / 1e12
     hbm_peak = _peak("hbm_gbs")
+    served = run_served(device, args.served_fp64) if not args.no_served else None
     cb = cpu_baseline(params, budget_s=args.cpu_budget) if not args.no_cpu else None
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
@@ -334,6 +335,7 @@ def run_ours(args) -> None:
                              "(no measured FP32 peak in MEASURED_PEAKS.json)",
                      "hbm": {"achieved": work["bytes"] / kern_s / 1e9, "peak": hbm_peak,
                              "unit": "GB/s", "frac": work["bytes"] / kern_s / 1e9 / hbm_peak}},
+        "served": served,
         "cpu_baseline": cb,
         "clocks": clocks,
         "setup_s": setup_s,
@@ -341,6 +343,71 @@ def run_ours(args) -> None:
     }
     print(json.dumps(line), flush=True)
     _barrier(dist)
+
+
+# ---- served request stream (continuous batching) ----------------------------------------------
+
+SERVED_COUNT, SERVED_MAX3D = 48, 256
+
+
+def _rel(a, b) -> float:
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def run_served(device: int, fp64_sample: int) -> dict:
+    """The served configuration: seeded Poisson arrivals of 70 % 2D (ny 1024-4096, 500-2000 slabs)
+    and 30 % 3D (lateral up to SERVED_MAX3D², 200-600 slabs) solves, microlens arrays or tilted
+    fibre facets, 2 iterations. A closed-loop pass (all requests at t = 0) measures capacity; the
+    open-loop pass offers 80 % of it as Poisson arrivals and reports p50/p99 latency (submit ->
+    result on the host) and solves/s; the plain FP64 per-solve path is timed on a sample."""
+    from bwpm_b200 import _core, workloads
+    from bwpm_b200.serve import Server, serve_stream
+
+    stream = workloads.request_stream(SERVED_COUNT, 1.0, seed=5, iterations=2,
+                                      max_lateral_3d=SERVED_MAX3D)
+    probs = [p for _, p in stream]
+    with Server(device) as srv:  # warm-up: module loading and first-use set-up of both engines
+        serve_stream(srv, [(0.0, p) for p in (next(p for p in probs if p.nx == 1),
+                                              next(p for p in probs if p.nx != 1))])
+    with Server(device) as srv:  # closed loop: capacity
+        _, wall = serve_stream(srv, [(0.0, p) for p in probs])
+    capacity = len(probs) / wall
+    rate = 0.8 * capacity
+    arrivals = workloads.poisson_arrivals(len(probs), rate, seed=5)
+    with Server(device) as srv:
+        res, wall = serve_stream(srv, list(zip(arrivals, probs)))
+        st = srv.stats()
+    lat = np.array([r["latency_ms"] for r in res])
+    # plain FP64 per-solve path (drop-in CudaSolver) on a sample; L2 error of the served results
+    rng = np.random.default_rng(9)
+    sample = [int(i) for i in rng.permutation(len(probs))[:fp64_sample]]
+    t64, errs = [], []
+    for i in sample:
+        p = probs[i]
+        s = _core.CudaSolver(*p.core_args(), device)
+        t0 = time.perf_counter()
+        r64 = s.run(p.field, p.iterations, [])
+        t64.append(time.perf_counter() - t0)
+        del s
+        for key in ("transmitted", "reflected"):
+            ref = r64[key][:, 0] if p.nx == 1 else r64[key]
+            errs.append(_rel(res[i][key], ref))
+    fp64_rate = 1.0 / float(np.mean(t64)) if t64 else None
+    value = len(probs) / wall
+    return {
+        "requests": len(probs), "n_3d": sum(p.nx != 1 for p in probs),
+        "solves_per_s": value, "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "offered_rate_hz": rate, "closed_loop_solves_per_s": capacity,
+        "fp64_plain_solves_per_s": fp64_rate, "fp64_sample": len(sample),
+        "speedup_vs_fp64_plain": value / fp64_rate if fp64_rate else None,
+        "l2_err_max": float(np.max(errs)) if errs else None,
+        "launch_groups": st["groups"], "max_concurrent": st["max_concurrent"],
+        "peak_device_bytes": st["peak_bytes"],
+        "note": "seeded Poisson stream at 80 % of the measured closed-loop capacity; 3D lateral "
+                f"sizes capped at {SERVED_MAX3D}^2 to bound host memory; latency = submit -> result "
+                "on the host; fp64 = per-solve FP64 CudaSolver on the sample, sequential",
+    }
 
 
 def prm_wl(prm: dict) -> float:
@@ -363,6 +430,8 @@ def main() -> None:
     ap.add_argument("--fp64-sample", type=int, default=6)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="target CPU seconds per core")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--served-fp64", type=int, default=3, help="FP64 sample of the served stream")
     ap.add_argument("--reduced", type=str, default="",
                     help="profiling only: COUNT,NZ_MAX,ITERATIONS (first COUNT solves, chains "
                          "capped); skips the FP64 and CPU comparisons")
@@ -371,6 +440,7 @@ def main() -> None:
         c, z, it = (int(v) for v in args.reduced.split(","))
         REDUCED.update(count=c, nz_max=z, iterations=it)
         args.no_cpu = True
+        args.no_served = True
         args.fp64_sample = 0
     if args.impl == "reference":
         run_reference(args)

@@ -32,7 +32,8 @@ constexpr int kClassThreads[] = {64, 128, 256, 512};
 constexpr int kGenericClasses = 4;
 constexpr int kMaxFixedLengths = 28;
 constexpr int kNumClasses = kGenericClasses + kMaxFixedLengths;  // ≥ kGenericClasses: fixed length
-constexpr int kTuneSlabs = 48;  // slabs per item in an autotuning run
+constexpr int kTuneScale = 8;     // autotuning runs keep 1/kTuneScale of every chain
+constexpr int kTuneMinSlabs = 8;
 
 // distinct lengths with compiled variants, increasing; class kGenericClasses + i serves entry i
 const std::vector<int>& fixed_lengths() {
@@ -61,10 +62,6 @@ std::vector<int> variants_of(int n) {
   return v;
 }
 
-// Autotuning results shared by every batch of the process: (length, log2 of the class's item
-// count) -> variant index.
-std::mutex g_tune_mu;
-std::map<std::pair<int, int>, int> g_tuned;
 
 // Twiddles of a variant: the stage twiddles of its per-CTA transform (N/C points); for a line
 // split over C CTAs followed by the cross twiddles w_N^{c·k1} (c < C, k1 < N/C), all (hi, lo).
@@ -84,15 +81,6 @@ std::vector<Tw<float>> variant_twiddles(const FixedVariant& f) {
       t.push_back(Tw<float>{h, cf{static_cast<float>(w.re - h.re), static_cast<float>(w.im - h.im)}});
     }
   return t;
-}
-
-int ilog2(int x) {
-  int r = 0;
-  while (x > 1) {
-    x >>= 1;
-    ++r;
-  }
-  return r;
 }
 
 // Operator table job: M/N of `kind` for (ñ_r, ñ_s), entry m00 (E_x) at out[0..2N) and m11 (E_y)
@@ -223,6 +211,7 @@ class Batch2DImpl final : public Batch2D {
     cudaDeviceProp prop{};
     check_cuda(cudaGetDeviceProperties(&prop, device), "props");
     sms_ = prop.multiProcessorCount;
+    check_cuda(cudaDeviceGetStreamPriorityRange(&prio_least_, &prio_greatest_), "priorities");
   }
   ~Batch2DImpl() override {
     if (exec_) cudaGraphExecDestroy(exec_);
@@ -298,7 +287,7 @@ class Batch2DImpl final : public Batch2D {
   }
 
  private:
-  void launch_classes(cudaStream_t origin);
+  void launch_classes(cudaStream_t origin, const R2Item* base = nullptr);
   void capture_graphs();
   void download();
   void use_variant(int c, int v);
@@ -313,6 +302,7 @@ class Batch2DImpl final : public Batch2D {
   int device_;
   OwnedStream main_;  // first: the pools below are stream-ordered allocations on it
   int sms_ = 148;
+  int prio_least_ = 0, prio_greatest_ = 0;  // launch priorities (greatest is numerically lowest)
   bool prepared_ = false;
   std::vector<HostSolve> solves_;
   std::vector<Item> items_;
@@ -747,10 +737,6 @@ void Batch2DImpl::prepare() {
         if (f->second < 0 || f->second >= static_cast<int>(vs.size()))
           throw invalid_argument("no variant " + std::to_string(f->second) + " for ny = " + std::to_string(n));
         pick = vs[f->second];
-      } else {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto t = g_tuned.find({n, ilog2(class_count_[c])});
-        if (t != g_tuned.end()) pick = t->second;
       }
       use_variant(c, pick);
       continue;
@@ -781,31 +767,46 @@ void Batch2DImpl::prepare() {
   if (use_graphs_) capture_graphs();
 }
 
-void Batch2DImpl::launch_classes(cudaStream_t origin) {
+void Batch2DImpl::launch_classes(cudaStream_t origin, const R2Item* base) {
+  if (!base) base = d_items_.ptr;
   check_cuda(cudaMemsetAsync(d_queue_.ptr, 0, kNumClasses * sizeof(int), origin), "queue reset");
   check_cuda(cudaEventRecord(ev0_, origin), "event");
   // longest chains first: classes in decreasing order of their first item's cost
   std::vector<int> order;
   for (int c = 0; c < kNumClasses; ++c)
     if (class_count_[c]) order.push_back(c);
-  std::sort(order.begin(), order.end(), [&](int a, int b) {
-    return items_[class_first_[a]].cost > items_[class_first_[b]].cost;
-  });
-  for (int c : order) {
+  // the longest item chain of a class: its first item's work over the CTAs that share a line
+  auto chain = [&](int c) {
+    const int cl = c >= kGenericClasses ? fixed_variants()[class_variant_[c]].cluster : 1;
+    return items_[class_first_[c]].cost / cl;
+  };
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return chain(a) > chain(b); });
+  for (std::size_t rank = 0; rank < order.size(); ++rank) {
+    const int c = order[rank];
     cudaStream_t s = streams_[c];
     check_cuda(cudaStreamWaitEvent(s, ev0_, 0), "wait");
-    const R2Item* items = d_items_.ptr + class_first_[c];
+    const R2Item* items = base + class_first_[c];
     int count = class_count_[c];
     int* q = d_queue_.ptr + c;
-    const dim3 grid(class_grid_[c]), block(class_threads_[c]);
+    // the longest chains first: their CTAs win free SMs over the other classes' CTAs
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = prio_greatest_ + std::min(static_cast<int>(rank), prio_least_ - prio_greatest_);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(class_grid_[c]);
+    cfg.blockDim = dim3(class_threads_[c]);
+    cfg.dynamicSmemBytes = class_smem_[c];
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     if (c >= kGenericClasses) {
       const Tw<float>* tw = d_twiddles_.ptr + variant_twbase_[class_variant_[c]];
       void* args[] = {&items, &count, &q, &tw};
-      check_cuda(cudaLaunchKernel(class_fn_[c], grid, block, args, class_smem_[c], s), "launch");
+      check_cuda(cudaLaunchKernelExC(&cfg, class_fn_[c], args), "launch");
     } else {
       R2Shared sh{d_plans_.ptr, d_twiddles_.ptr};
       void* args[] = {&items, &count, &q, &sh};
-      check_cuda(cudaLaunchKernel(class_fn_[c], grid, block, args, class_smem_[c], s), "launch");
+      check_cuda(cudaLaunchKernelExC(&cfg, class_fn_[c], args), "launch");
     }
     ++launches_;
     check_cuda(cudaEventRecord(class_done_[c], s), "event");
@@ -835,63 +836,65 @@ void Batch2DImpl::use_variant(int c, int v) {
   class_grid_[c] = std::min(class_count_[c], std::max(1, clusters)) * f.cluster;
 }
 
-// Times every variant of each fixed-length class on the class's own items, chains cut to
-// kTuneSlabs slabs and at most one iteration, and keeps the fastest (shared by later batches of
-// the process with the same length and item-count bucket). The cut runs write only into this
-// batch's own output and source buffers, which every full run rewrites before reading.
+// Autotuning by measurement of the batch itself.
+//
+// The whole batch runs with every chain scaled down (kTuneScale of its slabs, at least
+// kTuneMinSlabs, one iteration), all classes concurrently as in a real run, so SM sharing
+// between classes and co-resident CTAs are part of what is measured. Starting from the first
+// listed variants, coordinate descent over the fixed-length classes tries each alternative
+// variant and keeps it when the scaled batch gets faster; two rounds at most. The scaled runs
+// write only into this batch's own output and source buffers, which every full run rewrites
+// before reading.
 void Batch2DImpl::autotune() {
-  cudaEvent_t a, b;
-  check_cuda(cudaEventCreate(&a), "event");
-  check_cuda(cudaEventCreate(&b), "event");
+  std::vector<int> tunable;
   for (int c = kGenericClasses; c < kNumClasses; ++c) {
     if (!class_count_[c]) continue;
     const int n = fixed_lengths()[c - kGenericClasses];
-    const std::vector<int> vs = variants_of(n);
-    if (vs.size() < 2 || forced_.count(n)) continue;
-    const std::pair<int, int> key{n, ilog2(class_count_[c])};
-    {
-      std::lock_guard<std::mutex> lk(g_tune_mu);
-      if (g_tuned.count(key)) continue;
-    }
-    std::vector<R2Item> cut(h_items_.begin() + class_first_[c], h_items_.begin() + class_first_[c] + class_count_[c]);
-    for (auto& it : cut) {
-      it.nz = std::min(it.nz, kTuneSlabs);
-      it.iterations = std::min(it.iterations, 1);
-    }
-    DevBuf<R2Item> d_cut(cut.size(), main_.s);
-    d_cut.upload(cut.data(), cut.size());
-    float best = 1e30f;
-    int best_v = vs.front();
-    for (int v : vs) {
-      use_variant(c, v);
-      const R2Item* items = d_cut.ptr;
-      int count = class_count_[c];
-      int* q = d_queue_.ptr + c;
-      const Tw<float>* tw = d_twiddles_.ptr + variant_twbase_[v];
-      void* args[] = {&items, &count, &q, &tw};
-      float ms = 0;
-      for (int rep = 0; rep < 2; ++rep) {  // the first run warms caches and the instruction cache
-        check_cuda(cudaMemsetAsync(q, 0, sizeof(int), main_), "queue reset");
-        check_cuda(cudaEventRecord(a, main_), "event");
-        check_cuda(cudaLaunchKernel(class_fn_[c], dim3(class_grid_[c]), dim3(class_threads_[c]), args,
-                                    class_smem_[c], main_), "launch");
-        check_cuda(cudaEventRecord(b, main_), "event");
-        check_cuda(cudaEventSynchronize(b), "autotune");
-        check_cuda(cudaEventElapsedTime(&ms, a, b), "elapsed");
-        launches_ += 1;
-      }
-      if (ms < best) {
-        best = ms;
-        best_v = v;
-      }
-    }
-    use_variant(c, best_v);
-    class_tuned_ms_[c] = best;
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[key] = best_v;
+    if (variants_of(n).size() > 1 && !forced_.count(n)) tunable.push_back(c);
   }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  if (tunable.empty()) return;
+  std::vector<R2Item> cut(h_items_);
+  for (auto& it : cut) {
+    it.nz = std::min(it.nz, std::max(kTuneMinSlabs, it.nz / kTuneScale));
+    it.iterations = std::min(it.iterations, 1);
+  }
+  DevBuf<R2Item> d_cut(cut.size(), main_.s);
+  d_cut.upload(cut.data(), cut.size());
+  auto measure = [&] {
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {  // the first run warms caches and the instruction cache
+      check_cuda(cudaEventRecord(ev_start_, main_), "event");
+      launch_classes(main_, d_cut.ptr);
+      check_cuda(cudaEventRecord(ev_stop_, main_), "event");
+      check_cuda(cudaEventSynchronize(ev_stop_), "autotune");
+      float ms = 0;
+      check_cuda(cudaEventElapsedTime(&ms, ev_start_, ev_stop_), "elapsed");
+      if (rep > 0) best = std::min(best, ms);
+    }
+    return best;
+  };
+  float current = measure();
+  for (int round = 0; round < 2; ++round) {
+    bool changed = false;
+    for (int c : tunable) {
+      const int n = fixed_lengths()[c - kGenericClasses];
+      const int keep = class_variant_[c];
+      int best_v = keep;
+      for (int v : variants_of(n)) {
+        if (v == keep) continue;
+        use_variant(c, v);
+        const float t = measure();
+        if (t < 0.99f * current) {
+          current = t;
+          best_v = v;
+        }
+      }
+      use_variant(c, best_v);
+      changed |= best_v != keep;
+    }
+    if (!changed) break;
+  }
+  for (int c : tunable) class_tuned_ms_[c] = current;
 }
 
 void Batch2DImpl::capture_graphs() {
@@ -911,7 +914,7 @@ void Batch2DImpl::capture_graphs() {
              (const ItemIo*)d_io_.ptr, d_packed_out_.ptr);
     }
     check_cuda(cudaStreamEndCapture(main_, &g), "capture");
-    check_cuda(cudaGraphInstantiate(&exec, g, 0), "instantiate");
+    check_cuda(cudaGraphInstantiate(&exec, g, cudaGraphInstantiateFlagUseNodePriority), "instantiate");
     cudaGraphDestroy(g);
     kernels = static_cast<int>(launches_ - before);
     launches_ = before;

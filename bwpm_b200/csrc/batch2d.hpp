@@ -44,14 +44,15 @@ class Batch2D {
   virtual void prepare() = 0;
   // off: no CUDA graphs are captured at prepare (single-use batches); default on
   virtual void set_graphs(bool on) = 0;
-  // on: prepare() times the kernel variants of each fixed length on the batch's own items
-  // (chains cut short) and keeps the fastest; results are cached for the process. Default off
-  // (the first listed variant, or a cached choice).
+  // on: prepare() picks the kernel variant of each fixed length by timing the batch itself with
+  // every chain scaled down (all classes concurrently, as in a run): coordinate descent from
+  // the first listed variants. Default off (the first listed variant).
   virtual void set_autotune(bool on) = 0;
   // forces variant k (position among the variants of length n) for this batch
   virtual void set_variant(int n, int k) = 0;
   // class k (0 ≤ k < classes()): length (the largest for a generic class), threads, CTAs per
-  // line, variant position (−1: generic kernel), autotuned ms (0: not tuned); returns its items
+  // line, variant position (−1: generic kernel), scaled-batch time in ms of the autotuned
+  // choice (0: not tuned); returns its items
   virtual int class_info(int k, int& n, int& threads, int& cluster, int& variant, float& tuned_ms) const = 0;
   // enqueues one batched solve on the batch's stream and returns at once; ready() tells whether
   // it has finished (results then come from result())

@@ -110,6 +110,7 @@ class PlaneSolver final : public Solver {
   std::vector<cd> partial_host_;
   // launch shapes
   int thr2d_ = 32, thr_line3_ = 32;
+  int sms_ = 148;
   LaunchShape rows2_, rows3_, sel_, cols1_, cols2_, cols3_;
   std::int64_t launches_ = 0, gmres_applies_ = 0;
 };
@@ -118,6 +119,8 @@ template <typename T>
 LaunchShape PlaneSolver<T>::rows_shape(int ncomp, int rows_max) const {
   LaunchShape s;
   const std::size_t row_bytes = in_.nx * ncomp * sizeof(C);
+  // at most rows_max rows per CTA, and few enough for two CTAs per SM over the plane's rows
+  rows_max = std::min<int>(rows_max, std::max<int>(1, static_cast<int>(in_.ny) / (2 * sms_)));
   s.rows = static_cast<int>(std::max<std::size_t>(1, std::min<std::size_t>(rows_max, 49152 / row_bytes)));
   while (s.rows > 1 && threads_needed(hx_.plan, s.rows * ncomp) > kPlaneThreads) --s.rows;
   s.threads = std::max(64, threads_needed(hx_.plan, s.rows * ncomp));
@@ -131,6 +134,7 @@ LaunchShape PlaneSolver<T>::cols_shape(int ncomp, int tiles) const {
   LaunchShape s;
   const std::size_t col_bytes = in_.ny * ncomp * sizeof(C);
   int cols = std::max(1, static_cast<int>(64 / (ncomp * sizeof(C))));
+  cols = std::min(cols, std::max(1, static_cast<int>(in_.nx) / (2 * sms_)));  // two CTAs per SM
   while (cols > 1 && (col_bytes * cols * tiles > 98304 ||
                       threads_needed(hy_.plan, cols * ncomp) > kPlaneThreads))
     --cols;
@@ -152,6 +156,7 @@ void PlaneSolver<T>::setup() {
     if (l < 0 || static_cast<std::size_t>(l) >= in_.indices.size())
       throw invalid_argument("labels must index into `indices`");
   if (nn > (1u << 30)) throw invalid_argument("plane too large");
+  if (in_.indices.size() > 4096) throw invalid_argument("at most 4096 materials");
   // Born hosts per slab (cpp/src/solver.cpp:49-62)
   std::vector<int> host_of(in_.nz, -1);
   if (!in_.fluct.empty()) {
@@ -178,6 +183,7 @@ void PlaneSolver<T>::setup() {
   check_cuda(cudaSetDevice(in_.device), "cudaSetDevice");
   stream_.create();
   keep_pool_memory(in_.device);
+  check_cuda(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, in_.device), "SM count");
   hy_ = make_plan(static_cast<int>(in_.ny));
   hx_ = make_plan(static_cast<int>(in_.nx));
   auto upload_tw = [&](const HostPlan& hp, DevBuf<Tw<T>>& d) {
@@ -195,22 +201,44 @@ void PlaneSolver<T>::setup() {
   std::vector<std::int32_t> before(nn, -1);
   steps_.resize(in_.nz);
   std::vector<std::uint8_t> pid(nn);
+  // a label pair (r, s), r ∈ [−1, m), s ∈ [0, m), as one code (r + 1)·m + s: codes sort like the
+  // pairs, so a presence scan lists a step's pairs in the reference's std::set order
+  // (cpp/src/solver.cpp:389-390); per code: whether the indices differ (an interface)
+  const int m = static_cast<int>(in_.indices.size());
+  const std::size_t ncode = static_cast<std::size_t>(m + 1) * m;
+  std::vector<std::uint8_t> code_iface(ncode);
+  for (int r = -1; r < m; ++r)
+    for (int q = 0; q < m; ++q) {
+      const cd x = index_of(r), y = index_of(q);
+      code_iface[static_cast<std::size_t>(r + 1) * m + q] = x.re != y.re || x.im != y.im;
+    }
+  std::vector<std::uint32_t> code(nn), stamp(ncode, 0);
+  std::vector<int> code_id(ncode, -1);
   for (std::size_t p = 0; p < in_.nz; ++p) {
     const std::int32_t* a = p == 0 ? before.data() : in_.labels.data() + (p - 1) * nn;
     const std::int32_t* b = in_.labels.data() + p * nn;
-    std::set<std::pair<int, int>> ps;
-    for (std::size_t q = 0; q < nn; ++q) ps.emplace(a[q], b[q]);
+    const std::uint32_t mark = static_cast<std::uint32_t>(p) + 1;
+    std::vector<std::uint32_t> present;
+    for (std::size_t q = 0; q < nn; ++q) {
+      const std::uint32_t k = static_cast<std::uint32_t>(a[q] + 1) * m + b[q];
+      code[q] = k;
+      if (stamp[k] != mark) {
+        stamp[k] = mark;
+        present.push_back(k);
+      }
+    }
+    std::sort(present.begin(), present.end());
     StepInfo& st = steps_[p];
-    st.pairs.assign(ps.begin(), ps.end());
+    st.pairs.clear();
+    for (auto k : present) st.pairs.emplace_back(static_cast<int>(k / m) - 1, static_cast<int>(k % m));
     if (st.pairs.size() > 255) throw invalid_argument("more than 255 label pairs in one step");
     if (2 * st.pairs.size() > static_cast<std::size_t>(kMaxPasses))
       throw invalid_argument("too many label pairs in one step");
     if (st.pairs.size() > 1) {
-      std::map<std::pair<int, int>, int> id;
-      for (std::size_t i = 0; i < st.pairs.size(); ++i) id[st.pairs[i]] = static_cast<int>(i);
+      for (std::size_t i = 0; i < present.size(); ++i) code_id[present[i]] = static_cast<int>(i);
       std::uint64_t h = 1469598103934665603ULL;
       for (std::size_t q = 0; q < nn; ++q) {
-        pid[q] = static_cast<std::uint8_t>(id[{a[q], b[q]}]);
+        pid[q] = static_cast<std::uint8_t>(code_id[code[q]]);
         h = (h ^ pid[q]) * 1099511628211ULL;
       }
       long long found = -1;
@@ -227,10 +255,11 @@ void PlaneSolver<T>::setup() {
       st.pid_off = found;
     }
     st.iface_off = static_cast<long long>(iface_host.size());
-    for (std::size_t q = 0; q < nn; ++q) {
-      const cd x = index_of(a[q]), y = index_of(b[q]);
-      if (x.re != y.re || x.im != y.im) iface_host.push_back(static_cast<int>(q));
-    }
+    bool any_iface = false;
+    for (auto k : present) any_iface |= code_iface[k] != 0;
+    if (any_iface)
+      for (std::size_t q = 0; q < nn; ++q)
+        if (code_iface[code[q]]) iface_host.push_back(static_cast<int>(q));
     st.niface = static_cast<int>(iface_host.size() - st.iface_off);
     if (st.niface > 0 && !is2d()) {
       st.rowoff_off = static_cast<long long>(rowoff_host.size());

@@ -281,8 +281,13 @@ def _lens_array_profile(rng: np.random.Generator, coords: list[np.ndarray]) -> t
     return np.maximum(height, 0.0), n
 
 
-def request(rng: np.random.Generator, i: int, iterations: int = 2) -> Problem:
-    """One request of the served stream: 70 % 2D, 30 % 3D; microlens array or tilted facet."""
+SERVED_3D_LATERAL = (256, 384, 512, 768, 1024)
+
+
+def request(rng: np.random.Generator, i: int, iterations: int = 2,
+            max_lateral_3d: int = 1024) -> Problem:
+    """One request of the served stream: 70 % 2D, 30 % 3D; microlens array or tilted facet.
+    3D lateral sizes are drawn from SERVED_3D_LATERAL up to `max_lateral_3d`."""
     is2d = rng.uniform() < 0.7
     wl = 0.633
     lam = wl * 1e-3
@@ -294,7 +299,7 @@ def request(rng: np.random.Generator, i: int, iterations: int = 2) -> Problem:
         y = centred(ny, dy)
         coords = [y[:, None] * np.ones((1, 1))]
     else:
-        ny = nx = int(rng.choice([256, 384, 512, 768, 1024]))
+        ny = nx = int(rng.choice([v for v in SERVED_3D_LATERAL if v <= max_lateral_3d]))
         nz = int(rng.integers(200, 601))
         dy = dx = lam / 6
         dz = lam / 8
@@ -328,13 +333,19 @@ def request(rng: np.random.Generator, i: int, iterations: int = 2) -> Problem:
                    name=f"request_{i}_{kind}_{'2d' if is2d else '3d'}")
 
 
-def request_stream(count: int, rate_hz: float, seed: int = 5,
-                   iterations: int = 2) -> list[tuple[float, Problem]]:
+def request_stream(count: int, rate_hz: float, seed: int = 5, iterations: int = 2,
+                   max_lateral_3d: int = 1024) -> list[tuple[float, Problem]]:
     """Seeded Poisson arrivals: (arrival time in s, problem)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(count):
         t += float(rng.exponential(1.0 / rate_hz))
-        out.append((t, request(rng, i, iterations)))
+        out.append((t, request(rng, i, iterations, max_lateral_3d)))
     return out
+
+
+def poisson_arrivals(count: int, rate_hz: float, seed: int = 5) -> np.ndarray:
+    """Seeded Poisson arrival times (s) of `count` requests at `rate_hz`."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate_hz, size=count))

@@ -94,17 +94,17 @@ int bwpm_batch_add(bwpm_batch* b, size_t ny, double dy, double dz, double k0,
 
 /* Kernel choice per line length (before prepare). Lengths with compiled register-resident
  * kernels (bwpm_variant_count(ny) > 0) have one or more variants (threads per CTA, FFT radices,
- * CTAs per line). on = 1: prepare times every variant of each such length on the batch's own
- * items (chains cut short) and keeps the fastest; choices are kept for the process. Default:
- * the first variant, or a choice made earlier in the process. set_variant forces variant
- * `variant` (0-based) for length ny. */
+ * CTAs per line). on = 1: prepare picks them by timing the batch itself with every chain scaled
+ * down to 1/8 of its slabs and one iteration (all lengths concurrently, as in a run),
+ * coordinate descent from the first variants. Default: the first variant. set_variant forces
+ * variant `variant` (0-based) for length ny. */
 int bwpm_batch_set_autotune(bwpm_batch* b, int on);
 int bwpm_batch_set_variant(bwpm_batch* b, size_t ny, int variant);
 int bwpm_variant_count(size_t ny);
 
 /* Class k of a prepared batch (k < classes of bwpm_batch_stats): line length (the largest of a
  * generic class), threads per CTA, CTAs per line, variant (−1: generic kernel), work items and
- * the autotuned time of the chosen variant in ms (0: not tuned). */
+ * the scaled-batch time in ms of the autotuned choice (0: not tuned). */
 int bwpm_batch_class_info(const bwpm_batch* b, int64_t k, int64_t* ny, int64_t* threads,
                           int64_t* cluster, int64_t* variant, int64_t* items, float* tuned_ms);
 
@@ -142,7 +142,7 @@ void bwpm_batch_destroy(bwpm_batch* b);
  * arrival order while the device-memory budget holds, and launched in groups on the batched
  * resident engine; groups launched while others run share the GPU. 3D requests run through the
  * complex64 plane engine on their own streams. budget_bytes 0: 80 % of the free device memory;
- * max_groups / max_group_solves / max_3d ≤ 0: defaults (8, 64, 2). Destroying the server waits
+ * max_groups / max_group_solves / max_3d ≤ 0: defaults (8, 64, 4). Destroying the server waits
  * for every submitted request. */
 typedef struct bwpm_server bwpm_server;
 
