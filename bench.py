@@ -212,8 +212,9 @@ def _params():
     from bwpm_b200 import workloads
 
     prm = workloads.batch2d_params(COUNT, SEED)
-    if REDUCED:  # reduced case for profiling: fewer solves, shorter chains
-        prm = [dict(p, nz=min(p["nz"], REDUCED["nz_max"]), iterations=REDUCED["iterations"])
+    if REDUCED:  # reduced case for profiling: fewer solves, shorter chains, optionally one length
+        prm = [dict(p, nz=min(p["nz"], REDUCED["nz_max"]), iterations=REDUCED["iterations"],
+                    ny=REDUCED.get("ny") or p["ny"])
                for p in prm[: REDUCED["count"]]]
     return prm
 
@@ -433,12 +434,14 @@ def main() -> None:
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--served-fp64", type=int, default=3, help="FP64 sample of the served stream")
     ap.add_argument("--reduced", type=str, default="",
-                    help="profiling only: COUNT,NZ_MAX,ITERATIONS (first COUNT solves, chains "
-                         "capped); skips the FP64 and CPU comparisons")
+                    help="profiling only: COUNT,NZ_MAX,ITERATIONS[,NY] (first COUNT solves, chains "
+                         "capped, optionally all of length NY); skips the FP64, served and CPU "
+                         "comparisons")
     args = ap.parse_args()
     if args.reduced:
-        c, z, it = (int(v) for v in args.reduced.split(","))
-        REDUCED.update(count=c, nz_max=z, iterations=it)
+        vals = [int(v) for v in args.reduced.split(",")]
+        REDUCED.update(count=vals[0], nz_max=vals[1], iterations=vals[2],
+                       ny=vals[3] if len(vals) > 3 else None)
         args.no_cpu = True
         args.no_served = True
         args.fp64_sample = 0

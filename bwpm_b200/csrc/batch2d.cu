@@ -23,6 +23,7 @@
 #include "interface.cuh"
 #include "plan.hpp"
 #include "resident2d.cuh"
+#include "rgen.cuh"
 #include "variants.hpp"
 
 namespace bwpm {
@@ -31,7 +32,9 @@ namespace {
 constexpr int kClassThreads[] = {64, 128, 256, 512};
 constexpr int kGenericClasses = 4;
 constexpr int kMaxFixedLengths = 28;
-constexpr int kNumClasses = kGenericClasses + kMaxFixedLengths;  // ≥ kGenericClasses: fixed length
+constexpr int kMaxRt = 10;
+constexpr int kRtBase = kGenericClasses + kMaxFixedLengths;  // classes of the run-time-length kernels
+constexpr int kNumClasses = kRtBase + kMaxRt;  // [4, kRtBase): fixed lengths, then E values
 constexpr int kTuneScale = 8;     // autotuning runs keep 1/kTuneScale of every chain
 constexpr int kTuneMinSlabs = 8;
 
@@ -51,6 +54,37 @@ int fixed_length_index(int n) {
   const auto& l = fixed_lengths();
   auto it = std::lower_bound(l.begin(), l.end(), n);
   return it != l.end() && *it == n ? static_cast<int>(it - l.begin()) : -1;
+}
+
+// Radices (largest first) of a length n for a run-time-length kernel with E values per thread:
+// each radix divides E; empty if n has another prime factor or E lacks one of n's.
+std::vector<int> rt_radices(int n, int e) {
+  std::vector<int> r;
+  int m = n;
+  for (int p : {8, 4, 2, 5, 3}) {
+    if (e % p) continue;
+    while (m % p == 0) {
+      r.push_back(p);
+      m /= p;
+    }
+  }
+  if (m != 1) return {};
+  std::stable_sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
+  return r;
+}
+
+// Position in rt_variants() of the run-time-length kernel for length n: the smallest E (the most
+// threads) whose radices factor n, within the kernel's thread limit and the shared memory of
+// three padded lines; −1 if none.
+int rt_choice(int n) {
+  const auto& rv = rt_variants();
+  if (rt_smem_bytes(n) > 220 * 1024) return -1;
+  for (std::size_t i = 0; i < rv.size(); ++i) {
+    const int e = rv[i].e;
+    if (n % e || n / e > rg::rt_max_threads(e) || rt_radices(n, e).empty()) continue;
+    return static_cast<int>(i);
+  }
+  return -1;
 }
 
 // indices into fixed_variants() of the variants of length n (first: the default)
@@ -245,7 +279,11 @@ class Batch2DImpl final : public Batch2D {
   void set_autotune(bool on) override { autotune_ = on; }
   void set_variant(int n, int k) override {
     if (prepared_) throw invalid_argument("batch already prepared");
-    if (fixed_length_index(n) < 0) throw invalid_argument("ny = " + std::to_string(n) + " has no fixed variants");
+    if (k == -1) {  // the run-time-length kernel instead of the compiled ones
+      if (rt_choice(n) < 0) throw invalid_argument("ny = " + std::to_string(n) + " has no run-time-length kernel");
+    } else if (fixed_length_index(n) < 0) {
+      throw invalid_argument("ny = " + std::to_string(n) + " has no fixed variants");
+    }
     forced_[n] = k;
   }
   int class_info(int k, int& n, int& threads, int& cluster, int& variant, float& tuned_ms) const override {
@@ -253,11 +291,12 @@ class Batch2DImpl final : public Batch2D {
     for (int c = 0; c < kNumClasses; ++c) {
       if (!class_count_[c]) continue;
       if (seen++ != k) continue;
-      n = c >= kGenericClasses ? fixed_lengths()[c - kGenericClasses] : class_maxn_[c];
+      const bool fixed = c >= kGenericClasses && c < kRtBase;
+      n = fixed ? fixed_lengths()[c - kGenericClasses] : class_maxn_[c];
       threads = class_threads_[c];
-      cluster = c >= kGenericClasses ? fixed_variants()[class_variant_[c]].cluster : 1;
-      variant = -1;
-      if (c >= kGenericClasses) {
+      cluster = fixed ? fixed_variants()[class_variant_[c]].cluster : 1;
+      variant = c >= kRtBase ? -2 - (c - kRtBase) : -1;
+      if (fixed) {
         const std::vector<int> vs = variants_of(n);
         variant = static_cast<int>(std::find(vs.begin(), vs.end(), class_variant_[c]) - vs.begin());
       }
@@ -292,6 +331,11 @@ class Batch2DImpl final : public Batch2D {
   void download();
   void use_variant(int c, int v);
   void autotune();
+  // a compiled fixed-length kernel serves n (unless the run-time-length kernel was forced)
+  bool uses_fixed(int n) const {
+    auto f = forced_.find(n);
+    return fixed_length_index(n) >= 0 && !(f != forced_.end() && f->second == -1);
+  }
   template <typename K, typename... A>
   void launch(K kernel, dim3 grid, dim3 block, std::size_t smem, cudaStream_t s, A... args) {
     kernel<<<grid, block, smem, s>>>(args...);
@@ -376,22 +420,40 @@ void build_host(HostSolve& h) {
   std::vector<std::pair<int, int>> pairs;
   const bool refl = s.iterations > 0;
   h.steps.resize(s.nz);
+  // a label pair (r, s), r ∈ [−1, m), s ∈ [0, m), as the code (r + 1)·m + s (< 2^16 for m ≤ 255):
+  // codes sort like the pairs (the reference's std::set order, cpp/src/solver.cpp:389-390)
+  const int m = static_cast<int>(s.indices.size());
+  const std::size_t ncode = static_cast<std::size_t>(m + 1) * m;
+  std::vector<std::uint8_t> code_iface(ncode);
+  for (int r = -1; r < m; ++r)
+    for (int q = 0; q < m; ++q)
+      code_iface[static_cast<std::size_t>(r + 1) * m + q] = !same(index_of(r), index_of(q));
+  std::vector<std::uint16_t> code(n);
+  std::vector<std::uint32_t> stamp(ncode, 0), present;
+  std::vector<int> code_id(ncode, 0);
   for (int p = 0; p < s.nz; ++p) {
     const std::int32_t* a = p == 0 ? before.data() : s.labels.data() + static_cast<std::size_t>(p - 1) * n;
     const std::int32_t* b = s.labels.data() + static_cast<std::size_t>(p) * n;
-    pairs.clear();
+    const std::uint32_t mark = static_cast<std::uint32_t>(p) + 1;
+    present.clear();
     for (int q = 0; q < n; ++q) {
-      const std::pair<int, int> pr{a[q], b[q]};
-      if (std::find(pairs.begin(), pairs.end(), pr) == pairs.end()) pairs.push_back(pr);
+      const std::uint32_t k = static_cast<std::uint32_t>(a[q] + 1) * m + b[q];
+      code[q] = static_cast<std::uint16_t>(k);
+      if (stamp[k] != mark) {
+        stamp[k] = mark;
+        present.push_back(k);
+      }
     }
-    std::sort(pairs.begin(), pairs.end());
+    std::sort(present.begin(), present.end());
+    pairs.clear();
+    for (auto k : present) pairs.emplace_back(static_cast<int>(k / m) - 1, static_cast<int>(k % m));
     R2Step st{};
     st.pid = -1;
     if (pairs.size() > 1) {
+      for (std::size_t i = 0; i < present.size(); ++i) code_id[present[i]] = static_cast<int>(i);
       std::uint64_t hash = 1469598103934665603ULL;
       for (int q = 0; q < n; ++q) {
-        const std::pair<int, int> pr{a[q], b[q]};
-        pid[q] = static_cast<std::uint8_t>(std::lower_bound(pairs.begin(), pairs.end(), pr) - pairs.begin());
+        pid[q] = static_cast<std::uint8_t>(code_id[code[q]]);
         hash = (hash ^ pid[q]) * 1099511628211ULL;
       }
       long long found = -1;
@@ -408,8 +470,11 @@ void build_host(HostSolve& h) {
       st.pid = found;
     }
     st.iface = static_cast<long long>(h.iface.size());
-    for (int q = 0; q < n; ++q)
-      if (!same(index_of(a[q]), index_of(b[q]))) h.iface.push_back(q);
+    bool any_iface = false;
+    for (auto k : present) any_iface |= code_iface[k] != 0;
+    if (any_iface)
+      for (int q = 0; q < n; ++q)
+        if (code_iface[code[q]]) h.iface.push_back(q);
     st.niface = static_cast<int>(h.iface.size() - st.iface);
     // forward passes: T for every pair, then R where the indices differ (cpp/src/solver.cpp:396-397)
     st.fwd_off = static_cast<int>(h.passes.size());
@@ -477,14 +542,15 @@ void Batch2DImpl::prepare() {
     const int n = h.in.ny;
     if (seen_n.count(n)) continue;
     seen_n[n] = true;
-    if (fixed_length_index(n) >= 0) {
+    if (uses_fixed(n)) {
       for (int v : variants_of(n)) {
         variant_twbase_[v] = static_cast<int>(tw.size());
         for (auto& t : variant_twiddles(fixed_variants()[v])) tw.push_back(t);
       }
       continue;
     }
-    HostPlan hp = make_plan(n);
+    const int rt = rt_choice(n);
+    HostPlan hp = rt >= 0 ? make_plan_radices(n, rt_radices(n, rt_variants()[rt].e)) : make_plan(n);
     const int base = static_cast<int>(tw.size());
     for (auto& t : twiddles_for<float>(hp)) tw.push_back(t);
     for (int st = 0; st < hp.plan.nstages; ++st) hp.plan.twoff[st] += base;
@@ -519,8 +585,10 @@ void Batch2DImpl::prepare() {
       for (int q = 0; q < n && !any; ++q) any = h.in.field[2 * q + c].re != 0.0 || h.in.field[2 * q + c].im != 0.0;
       if (!any) continue;
       int cls = 0;
-      if (fixed_length_index(n) >= 0) {
+      if (uses_fixed(n)) {
         cls = kGenericClasses + fixed_length_index(n);
+      } else if (rt_choice(n) >= 0) {
+        cls = kRtBase + rt_choice(n);
       } else {
         const int want = threads_needed(plans[plan_of[n]], 1, kR2Ept);
         if (want > kClassThreads[kGenericClasses - 1])
@@ -727,7 +795,7 @@ void Batch2DImpl::prepare() {
   set_attr((const void*)k_resident2d<512>);
   for (int c = 0; c < kNumClasses; ++c) {
     if (!class_count_[c]) continue;
-    if (c >= kGenericClasses) {
+    if (c >= kGenericClasses && c < kRtBase) {
       const int n = fixed_lengths()[c - kGenericClasses];
       const std::vector<int> vs = variants_of(n);
       for (int v : vs) set_attr(fixed_variants()[v].fn);
@@ -741,10 +809,20 @@ void Batch2DImpl::prepare() {
       use_variant(c, pick);
       continue;
     }
-    const void* k = c == 0 ? (const void*)k_resident2d<64> : c == 1 ? (const void*)k_resident2d<128>
-                    : c == 2 ? (const void*)k_resident2d<256> : (const void*)k_resident2d<512>;
-    const int threads = kClassThreads[c];
-    class_smem_[c] = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+    const void* k;
+    int threads;
+    if (c >= kRtBase) {  // run-time-length kernel: threads of the class's longest line
+      const RtVariant& r = rt_variants()[c - kRtBase];
+      k = r.fn;
+      threads = (class_maxn_[c] / r.e + 31) / 32 * 32;
+      class_smem_[c] = rt_smem_bytes(class_maxn_[c]);
+      set_attr(k);
+    } else {
+      k = c == 0 ? (const void*)k_resident2d<64> : c == 1 ? (const void*)k_resident2d<128>
+          : c == 2 ? (const void*)k_resident2d<256> : (const void*)k_resident2d<512>;
+      threads = kClassThreads[c];
+      class_smem_[c] = 3 * static_cast<std::size_t>(class_maxn_[c]) * sizeof(cf);
+    }
     int per_sm = 0;
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, class_smem_[c]), "occupancy");
     per_sm = std::max(1, per_sm);
@@ -777,7 +855,7 @@ void Batch2DImpl::launch_classes(cudaStream_t origin, const R2Item* base) {
     if (class_count_[c]) order.push_back(c);
   // the longest item chain of a class: its first item's work over the CTAs that share a line
   auto chain = [&](int c) {
-    const int cl = c >= kGenericClasses ? fixed_variants()[class_variant_[c]].cluster : 1;
+    const int cl = c >= kGenericClasses && c < kRtBase ? fixed_variants()[class_variant_[c]].cluster : 1;
     return items_[class_first_[c]].cost / cl;
   };
   std::sort(order.begin(), order.end(), [&](int a, int b) { return chain(a) > chain(b); });
@@ -799,7 +877,7 @@ void Batch2DImpl::launch_classes(cudaStream_t origin, const R2Item* base) {
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (c >= kGenericClasses) {
+    if (c >= kGenericClasses && c < kRtBase) {
       const Tw<float>* tw = d_twiddles_.ptr + variant_twbase_[class_variant_[c]];
       void* args[] = {&items, &count, &q, &tw};
       check_cuda(cudaLaunchKernelExC(&cfg, class_fn_[c], args), "launch");
@@ -847,7 +925,7 @@ void Batch2DImpl::use_variant(int c, int v) {
 // before reading.
 void Batch2DImpl::autotune() {
   std::vector<int> tunable;
-  for (int c = kGenericClasses; c < kNumClasses; ++c) {
+  for (int c = kGenericClasses; c < kRtBase; ++c) {
     if (!class_count_[c]) continue;
     const int n = fixed_lengths()[c - kGenericClasses];
     if (variants_of(n).size() > 1 && !forced_.count(n)) tunable.push_back(c);

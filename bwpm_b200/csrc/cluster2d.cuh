@@ -38,6 +38,24 @@ struct Shape {
   static_assert(N % C == 0 && M % NT == 0 && E % C == 0, "cluster shape");
 };
 
+// Shared memory of a cluster kernel: three padded lines and two exchange buffers of M points,
+// then (16-byte aligned) the CTA's twiddles: the M − 1 stage twiddles, the forward cross
+// twiddles w_N^{c·k1} (k1 < M) and the inverse ones of its spectral block (C·M/C), loaded once
+// per CTA. Lengths whose twiddles do not fit read them from global memory (L2).
+template <int N, int C>
+__host__ __device__ constexpr std::size_t cluster_lines_bytes() {
+  return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * (N / C)) * sizeof(cf) + 15) / 16 * 16;
+}
+template <int N, int C>
+__host__ __device__ constexpr bool cluster_tw_in_smem() {
+  return r2c::cluster_lines_bytes<N, C>() + static_cast<std::size_t>(3 * (N / C) - 1) * sizeof(Tw<float>) <= 220 * 1024;
+}
+template <int N, int C>
+__host__ __device__ constexpr std::size_t cluster_smem_bytes() {
+  return r2c::cluster_lines_bytes<N, C>() +
+         (r2c::cluster_tw_in_smem<N, C>() ? static_cast<std::size_t>(3 * (N / C) - 1) * sizeof(Tw<float>) : 0);
+}
+
 // spectral index of slot s (= k2·EB + i) of thread t in CTA c
 template <int N, int C, int NT>
 __device__ __forceinline__ int kspec(int s, int t, int c) {
@@ -57,14 +75,15 @@ __device__ __forceinline__ int qreal(int j, int t, int c) {
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
                                         cf* const (&xb)[2], int& xphase, const Tw<float>* tw,
-                                        const Tw<float>* xtw, int t, int c, cg::cluster_group& cl) {
+                                        const Tw<float>* xf, const Tw<float>* xi, int t, int c,
+                                        cg::cluster_group& cl) {
   using S = Shape<N, C, NT>;
   rf::fft<-1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
   cf* x = xb[xphase];
 #pragma unroll
   for (int j = 0; j < S::E; ++j) {
     const int k1 = t + j * NT;
-    x[k1] = c == 0 ? v[j] : twmul<-1>(v[j], xtw[c * S::M + k1]);
+    x[k1] = c == 0 ? v[j] : twmul<-1>(v[j], xf[k1]);
   }
   cl.sync();
 #pragma unroll
@@ -84,18 +103,22 @@ __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
                                         cf* const (&xb)[2], int& xphase, const Tw<float>* tw,
-                                        const Tw<float>* xtw, int t, int c, cg::cluster_group& cl) {
+                                        const Tw<float>* xf, const Tw<float>* xi, int t, int c,
+                                        cg::cluster_group& cl) {
   using S = Shape<N, C, NT>;
   cf* x = xb[xphase];
 #pragma unroll
   for (int i = 0; i < S::EB; ++i) {
-    const int k1l = i * NT + t, k1 = c * S::MB + k1l;
+    const int k1l = i * NT + t;
     cf u[C];
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) u[k2] = v[k2 * S::EB + i];
     rf::dft<+1, C>(u);
+    // inverse cross twiddles: d·MB + k1l staged in shared memory, else d·M + c·MB + k1l in the
+    // global table (xi then points at its c·MB entry)
+    constexpr int xs = r2c::cluster_tw_in_smem<N, C>() ? S::MB : S::M;
 #pragma unroll
-    for (int d = 0; d < C; ++d) x[d * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xtw[d * S::M + k1]);
+    for (int d = 0; d < C; ++d) x[d * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xi[d * xs + k1l]);
   }
   cl.sync();
 #pragma unroll
@@ -159,7 +182,8 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
                                      cf* b0, cf* b1, int& phase, cf* const (&xb)[2], int& xphase,
                                      const R2Item& it, const R2Step& st, bool backward, bool reflect,
                                      cf* store, const cf* add, const Tw<float>* tw,
-                                     const Tw<float>* xtw, int t, int c, cg::cluster_group& cl) {
+                                     const Tw<float>* xf, const Tw<float>* xi, int t, int c,
+                                     cg::cluster_group& cl) {
   using Sh = Shape<N, C, NT>;
   constexpr int E = Sh::E;
   const int off = backward ? st.bwd_off : st.fwd_off;
@@ -167,7 +191,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
   const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
-  forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+  forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
   if (npass == 1) {
     const cf* m = it.tables + it.passes[off].tab;
 #pragma unroll
@@ -175,7 +199,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
       const int k = kspec<N, C, NT>(j, t, c);
       v[j] = pmul(v[j], m[k], m[N + k]);
     }
-    inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+    inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
     if (it.mask)
 #pragma unroll
       for (int j = 0; j < E; ++j) {
@@ -193,7 +217,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
         const int k = kspec<N, C, NT>(j, t, c);
         v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
       }
-      inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+      inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
       if (!ps.refl) {
 #pragma unroll
         for (int j = 0; j < E; ++j) {
@@ -241,7 +265,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
 template <int N, int C, int NT, class RADS>
 __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
     k_resident2d_cluster(const R2Item* __restrict__ items, int nitems, int* queue,
-                         const Tw<float>* __restrict__ tw) {
+                         const Tw<float>* __restrict__ tw_global) {
   using S = r2c::Shape<N, C, NT>;
   constexpr int E = S::E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -255,7 +279,26 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   r2c::cg::cluster_group cl = r2c::cg::this_cluster();
   const int t = threadIdx.x;
   const int c = static_cast<int>(cl.block_rank());
-  const Tw<float>* xtw = tw + (S::M - 1);
+  // global layout: M − 1 stage twiddles, then w_N^{c·k1} at (M − 1) + c·M + k1
+  const Tw<float>* xg = tw_global + (S::M - 1);
+  const Tw<float>* tw = tw_global;
+  const Tw<float>* xf = xg + c * S::M;   // forward: this CTA's c, every k1
+  const Tw<float>* xi = nullptr;         // inverse: entry d·MB + k1l for k1 = c·MB + k1l
+  Tw<float>* xi_s = nullptr;
+  if constexpr (r2c::cluster_tw_in_smem<N, C>()) {
+    Tw<float>* tws = reinterpret_cast<Tw<float>*>(smem_raw + r2c::cluster_lines_bytes<N, C>());
+    Tw<float>* xfs = tws + (S::M - 1);
+    xi_s = xfs + S::M;
+    for (int i = t; i < S::M - 1; i += NT) tws[i] = tw_global[i];
+    for (int i = t; i < S::M; i += NT) xfs[i] = xf[i];
+    for (int i = t; i < S::M; i += NT) xi_s[i] = xg[(i / S::MB) * S::M + c * S::MB + i % S::MB];
+    __syncthreads();
+    tw = tws;
+    xf = xfs;
+    xi = xi_s;
+  } else {
+    xi = xg + c * S::MB;
+  }
   int phase = 0, xphase = 0;
   for (;;) {
     if (c == 0 && t == 0) s_item = atomicAdd(queue, 1);
@@ -271,7 +314,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
     const int iters = it.iterations > 0 ? it.iterations : 1;
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = it.input[r2c::qreal<N, C, NT>(j, t, c)];
-    r2c::forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+    r2c::forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
     {
       const double pin = r2c::flux<N, C, NT>(v, it.w_in, s_red, &s_part, t, c, cl);
       if (c == 0 && t == 0) it.energy[2 * iters] = pin;
@@ -295,7 +338,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
         r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, xb, xphase, it, st, backward, reflect,
-                                  store, add, tw, xtw, t, c, cl);
+                                  store, add, tw, xf, xi, t, c, cl);
       }
       cf* dst = backward ? it.reflected : it.transmitted;
 #pragma unroll
@@ -303,7 +346,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
       if (it.iterations == 0) break;
 #pragma unroll
       for (int j = 0; j < E; ++j) out[j] = v[j];
-      r2c::forward<N, C, NT, RADS>(out, b0, b1, phase, xb, xphase, tw, xtw, t, c, cl);
+      r2c::forward<N, C, NT, RADS>(out, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
       const double fl = r2c::flux<N, C, NT>(out, backward ? it.w_in : it.w_out, s_red, &s_part, t, c, cl);
       if (c == 0 && t == 0) it.energy[2 * iter + (backward ? 1 : 0)] = fl;
     }

@@ -364,10 +364,25 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
   }
 }
 
+// Shared memory of a fixed-length kernel: three padded lines, then (16-byte aligned) the N − 1
+// stage twiddles of the class when they fit, loaded once per CTA; else they are read from
+// global memory (L2).
+__host__ __device__ constexpr std::size_t lines_bytes(int n, int lines) {
+  return (static_cast<std::size_t>(lines) * rf::padded(n) * sizeof(cf) + 15) / 16 * 16;
+}
+template <int N>
+__host__ __device__ constexpr bool fixed_tw_in_smem() {
+  return lines_bytes(N, 3) + static_cast<std::size_t>(N - 1) * sizeof(Tw<float>) <= 220 * 1024;
+}
+template <int N>
+__host__ __device__ constexpr std::size_t fixed_smem_bytes() {
+  return lines_bytes(N, 3) + (fixed_tw_in_smem<N>() ? static_cast<std::size_t>(N - 1) * sizeof(Tw<float>) : 0);
+}
+
 template <int N, int NT, class RADS>
 __global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __restrict__ items,
                                                          int nitems, int* queue,
-                                                         const Tw<float>* __restrict__ tw) {
+                                                         const Tw<float>* __restrict__ tw_global) {
   constexpr int E = N / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cf* b0 = reinterpret_cast<cf*>(smem_raw);
@@ -376,6 +391,13 @@ __global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __rest
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
   const int t = threadIdx.x;
+  const Tw<float>* tw = tw_global;
+  if constexpr (fixed_tw_in_smem<N>()) {
+    Tw<float>* tws = reinterpret_cast<Tw<float>*>(smem_raw + lines_bytes(N, 3));
+    for (int i = t; i < N - 1; i += NT) tws[i] = tw_global[i];
+    __syncthreads();
+    tw = tws;
+  }
   int phase = 0;
   for (;;) {
     if (t == 0) s_item = atomicAdd(queue, 1);

@@ -80,7 +80,9 @@ class ServerImpl final : public Server {
     opt_.max_groups = std::max(1, opt_.max_groups);
     opt_.max_group_solves = std::max(1, opt_.max_group_solves);
     opt_.max_3d = std::max(1, opt_.max_3d);
-    for (int i = 0; i < std::max(1, opt_.prep_threads); ++i) threads_.emplace_back([this] { prep_loop(); });
+    if (opt_.prep_threads <= 0)
+      opt_.prep_threads = static_cast<int>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    for (int i = 0; i < opt_.prep_threads; ++i) threads_.emplace_back([this] { prep_loop(); });
     threads_.emplace_back([this] { launch_loop(); });
     threads_.emplace_back([this] { complete_loop(); });
     for (int i = 0; i < opt_.max_3d; ++i) threads_.emplace_back([this] { run3d_loop(); });

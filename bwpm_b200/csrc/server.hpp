@@ -17,7 +17,7 @@ struct ServerOptions {
   int max_groups = 8;            // 2D launch groups in flight
   int max_group_solves = 64;     // solves per 2D launch group
   int max_3d = 4;                // 3D solves in flight
-  int prep_threads = 4;          // host preparation workers
+  int prep_threads = 0;          // host preparation workers; 0: one per host core, at most 16
 };
 
 struct ServedResult {

@@ -22,6 +22,14 @@ struct FixedVariant {
 // every compiled variant, grouped by length in increasing order
 const std::vector<FixedVariant>& fixed_variants();
 
+// Run-time-length kernels: E values per thread, any length n = E·nt whose radices (2, 3, 4, 5,
+// 8) all divide E, nt ≤ 512 threads (256 for E > 8); ordered by increasing E.
+struct RtVariant {
+  int e;
+  const void* fn;
+};
+const std::vector<RtVariant>& rt_variants();
+
 // parts of the registry compiled in separate translation units
 void add_variants_small(std::vector<FixedVariant>& v);
 void add_variants_large(std::vector<FixedVariant>& v);

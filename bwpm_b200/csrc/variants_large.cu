@@ -10,15 +10,13 @@ using rf::Radices;
 
 template <int N, int NT, int... R>
 FixedVariant fixed() {
-  return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>,
-          3 * static_cast<std::size_t>(rf::padded(N)) * sizeof(cf)};
+  return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>, fixed_smem_bytes<N>()};
 }
-// one line over a cluster of C CTAs: 3 transform lines of M = N/C points + 2 exchange buffers
+// one line over a cluster of C CTAs
 template <int N, int C, int NT, int... R>
 FixedVariant cluster() {
-  constexpr int M = N / C;
   return {N, NT, C, {R...}, (const void*)k_resident2d_cluster<N, C, NT, Radices<R...>>,
-          (3 * static_cast<std::size_t>(rf::padded(M)) + 2 * static_cast<std::size_t>(M)) * sizeof(cf)};
+          r2c::cluster_smem_bytes<N, C>()};
 }
 }  // namespace
 

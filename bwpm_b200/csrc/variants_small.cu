@@ -9,8 +9,7 @@ using rf::Radices;
 
 template <int N, int NT, int... R>
 FixedVariant fixed() {
-  return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>,
-          3 * static_cast<std::size_t>(rf::padded(N)) * sizeof(cf)};
+  return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>, fixed_smem_bytes<N>()};
 }
 }  // namespace
 

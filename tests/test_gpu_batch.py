@@ -203,3 +203,39 @@ def test_autotuned_batch_equals_forced_variant():
     forced.run()
     for i, j in zip(ids, fids):
         assert np.array_equal(b.result(i)["transmitted"], forced.result(j)["transmitted"])
+
+
+@pytest.mark.parametrize("n", [1000, 1125, 1200, 1944, 2160, 2187, 3645, 4000, 3125])
+def test_runtime_length_kernels_match_fp64(n):
+    """Lengths without a compiled kernel: the run-time-length register kernels (E values per
+    thread, radices 2/3/4/5/8 dividing E), or the generic kernel (3125 = 5^5), against FP64."""
+    from bwpm_b200.batch import Batch2D
+
+    p = _variant_problem(n)
+    ref = _fp64(p)
+    b = Batch2D()
+    i = b.add_problem(p)
+    b.run()
+    cls = b.classes()[0]
+    assert cls["variant"] <= -1 and cls["ny"] == n
+    assert (cls["variant"] == -1) == (n == 3125), cls  # −1: generic kernel, ≤ −2: run-time length
+    r = b.result(i)
+    assert rel_l2(r["transmitted"], ref["transmitted"][:, 0]) < L2_C64, cls
+    assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64, cls
+
+
+@pytest.mark.parametrize("n", [1024, 2048])
+def test_runtime_length_kernel_forced_at_a_fixed_length(n):
+    """set_variant(n, −1): the run-time-length kernel serves a length that has compiled ones."""
+    from bwpm_b200.batch import Batch2D
+
+    p = _variant_problem(n)
+    ref = _fp64(p)
+    b = Batch2D()
+    b.set_variant(n, -1)
+    i = b.add_problem(p)
+    b.run()
+    assert b.classes()[0]["variant"] <= -2
+    r = b.result(i)
+    assert rel_l2(r["transmitted"], ref["transmitted"][:, 0]) < L2_C64
+    assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64
