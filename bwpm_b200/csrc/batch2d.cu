@@ -35,7 +35,7 @@ constexpr int kMaxFixedLengths = 28;
 constexpr int kMaxRt = 10;
 constexpr int kRtBase = kGenericClasses + kMaxFixedLengths;  // classes of the run-time-length kernels
 constexpr int kNumClasses = kRtBase + kMaxRt;  // [4, kRtBase): fixed lengths, then E values
-constexpr int kTuneScale = 8;     // autotuning runs keep 1/kTuneScale of every chain
+constexpr int kTuneScale = 4;     // autotuning runs keep 1/kTuneScale of every chain
 constexpr int kTuneMinSlabs = 8;
 
 // distinct lengths with compiled variants, increasing; class kGenericClasses + i serves entry i
@@ -938,20 +938,37 @@ void Batch2DImpl::autotune() {
   }
   DevBuf<R2Item> d_cut(cut.size(), main_.s);
   d_cut.upload(cut.data(), cut.size());
+  std::vector<long long> clk(2 * items_.size());
+  // one measurement: the scaled batch's time (median of three runs after a warm run) and, per
+  // class, its SM time in that run (Σ item latency × CTAs per item)
+  struct Meas {
+    float ms;
+    std::vector<double> class_sm;
+  };
   auto measure = [&] {
-    float best = 1e30f;
-    for (int rep = 0; rep < 3; ++rep) {  // the first run warms caches and the instruction cache
+    std::vector<float> runs;
+    for (int rep = 0; rep < 4; ++rep) {
       check_cuda(cudaEventRecord(ev_start_, main_), "event");
       launch_classes(main_, d_cut.ptr);
       check_cuda(cudaEventRecord(ev_stop_, main_), "event");
       check_cuda(cudaEventSynchronize(ev_stop_), "autotune");
       float ms = 0;
       check_cuda(cudaEventElapsedTime(&ms, ev_start_, ev_stop_), "elapsed");
-      if (rep > 0) best = std::min(best, ms);
+      if (rep > 0) runs.push_back(ms);
     }
-    return best;
+    std::sort(runs.begin(), runs.end());
+    Meas m{runs[runs.size() / 2], std::vector<double>(kNumClasses, 0.0)};
+    check_cuda(cudaMemcpyAsync(clk.data(), d_clock_.ptr, clk.size() * sizeof(long long),
+                               cudaMemcpyDeviceToHost, main_), "clocks");
+    check_cuda(cudaStreamSynchronize(main_), "clocks");
+    for (std::size_t k = 0; k < items_.size(); ++k) {
+      const int c = items_[k].cls;
+      const int cl = c >= kGenericClasses && c < kRtBase ? fixed_variants()[class_variant_[c]].cluster : 1;
+      m.class_sm[c] += static_cast<double>(clk[2 * k + 1] - clk[2 * k]) * 1e-6 * cl;
+    }
+    return m;
   };
-  float current = measure();
+  Meas current = measure();
   for (int round = 0; round < 2; ++round) {
     bool changed = false;
     for (int c : tunable) {
@@ -961,8 +978,12 @@ void Batch2DImpl::autotune() {
       for (int v : variants_of(n)) {
         if (v == keep) continue;
         use_variant(c, v);
-        const float t = measure();
-        if (t < 0.99f * current) {
+        const Meas t = measure();
+        // clearly faster batch, or an equal batch (within the run-to-run spread) whose class
+        // needs clearly less SM time (frees SMs for the other classes)
+        const bool faster = t.ms < 0.985f * current.ms;
+        const bool leaner = t.ms < 1.01f * current.ms && t.class_sm[c] < 0.8 * current.class_sm[c];
+        if (faster || leaner) {
           current = t;
           best_v = v;
         }
@@ -972,7 +993,7 @@ void Batch2DImpl::autotune() {
     }
     if (!changed) break;
   }
-  for (int c : tunable) class_tuned_ms_[c] = current;
+  for (int c : tunable) class_tuned_ms_[c] = current.ms;
 }
 
 void Batch2DImpl::capture_graphs() {

@@ -39,21 +39,14 @@ struct Shape {
 };
 
 // Shared memory of a cluster kernel: three padded lines and two exchange buffers of M points,
-// then (16-byte aligned) the CTA's twiddles: the M − 1 stage twiddles, the forward cross
-// twiddles w_N^{c·k1} (k1 < M) and the inverse ones of its spectral block (C·M/C), loaded once
-// per CTA. Lengths whose twiddles do not fit read them from global memory (L2).
+// then the mask of the CTA's points (M hi values, M lo values).
 template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_lines_bytes() {
   return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * (N / C)) * sizeof(cf) + 15) / 16 * 16;
 }
 template <int N, int C>
-__host__ __device__ constexpr bool cluster_tw_in_smem() {
-  return r2c::cluster_lines_bytes<N, C>() + static_cast<std::size_t>(3 * (N / C) - 1) * sizeof(Tw<float>) <= 220 * 1024;
-}
-template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_smem_bytes() {
-  return r2c::cluster_lines_bytes<N, C>() +
-         (r2c::cluster_tw_in_smem<N, C>() ? static_cast<std::size_t>(3 * (N / C) - 1) * sizeof(Tw<float>) : 0);
+  return cluster_lines_bytes<N, C>() + 2 * static_cast<std::size_t>(N / C) * sizeof(float);
 }
 
 // spectral index of slot s (= k2·EB + i) of thread t in CTA c
@@ -114,11 +107,9 @@ __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) u[k2] = v[k2 * S::EB + i];
     rf::dft<+1, C>(u);
-    // inverse cross twiddles: d·MB + k1l staged in shared memory, else d·M + c·MB + k1l in the
-    // global table (xi then points at its c·MB entry)
-    constexpr int xs = r2c::cluster_tw_in_smem<N, C>() ? S::MB : S::M;
+    // inverse cross twiddle w_N^{−d·k1}, k1 = c·MB + k1l: entry d·M + k1l of xi = table + c·MB
 #pragma unroll
-    for (int d = 0; d < C; ++d) x[d * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xi[d * xs + k1l]);
+    for (int d = 0; d < C; ++d) x[d * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xi[d * S::M + k1l]);
   }
   cl.sync();
 #pragma unroll
@@ -176,41 +167,51 @@ __device__ __forceinline__ double flux(const cf (&v)[Shape<N, C, NT>::E], const 
   return total;
 }
 
-// One slab step of the CTA's share of an item (cf. r2f_step).
+// One slab step of the CTA's share of an item (cf. r2f_step: prefetched records and operator
+// values; mk: the mask of the CTA's points in shared memory, M hi then M lo values, or null).
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&out)[Shape<N, C, NT>::E],
                                      cf* b0, cf* b1, int& phase, cf* const (&xb)[2], int& xphase,
-                                     const R2Item& it, const R2Step& st, bool backward, bool reflect,
-                                     cf* store, const cf* add, const Tw<float>* tw,
-                                     const Tw<float>* xf, const Tw<float>* xi, int t, int c,
-                                     cg::cluster_group& cl) {
+                                     const R2Item& it, const R2Step& st, const R2Pass& p0,
+                                     R2Next& nx, int next_p, bool next_backward, bool backward,
+                                     bool reflect, cf* store, const cf* add, const float* mk,
+                                     const Tw<float>* tw, const Tw<float>* xf, const Tw<float>* xi,
+                                     int t, int c, cg::cluster_group& cl) {
   using Sh = Shape<N, C, NT>;
-  constexpr int E = Sh::E;
+  constexpr int E = Sh::E, M = Sh::M;
   const int off = backward ? st.bwd_off : st.fwd_off;
   const int ntp = backward ? st.bwd_t : st.fwd_t;
   const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
-  forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+  if (next_p >= 0) nx.st = it.steps[next_p];
   if (npass == 1) {
-    const cf* m = it.tables + it.passes[off].tab;
+    const cf* m = it.tables + p0.tab;
+    cf th[E], tl[E];  // in flight during the forward transform
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int k = kspec<N, C, NT>(j, t, c);
-      v[j] = pmul(v[j], m[k], m[N + k]);
+      th[j] = m[k];
+      tl[j] = m[N + k];
     }
+    forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = pmul(v[j], th[j], tl[j]);
     inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
-    if (it.mask)
+    if (mk)
 #pragma unroll
       for (int j = 0; j < E; ++j) {
-        const int q = qreal<N, C, NT>(j, t, c);
-        v[j] = mask_mul(v[j], it.mask[q], it.mask[N + q]);
+        const int m = t + j * NT;
+        v[j] = mask_mul(v[j], mk[m], mk[M + m]);
       }
   } else {
+    forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
 #pragma unroll
     for (int j = 0; j < E; ++j) S[rf::pad(t + j * NT)] = v[j];
     for (int p = 0; p < npass; ++p) {
-      const R2Pass ps = it.passes[off + p];
+      const R2Pass ps = p == 0 ? p0 : it.passes[off + p];
       const cf* m = it.tables + ps.tab;
 #pragma unroll
       for (int j = 0; j < E; ++j) {
@@ -221,8 +222,8 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
       if (!ps.refl) {
 #pragma unroll
         for (int j = 0; j < E; ++j) {
-          const int q = qreal<N, C, NT>(j, t, c);
-          if (!pid || pid[q] == ps.pair) out[j] = it.mask ? mask_mul(v[j], it.mask[q], it.mask[N + q]) : v[j];
+          const int q = qreal<N, C, NT>(j, t, c), ml = t + j * NT;
+          if (!pid || pid[q] == ps.pair) out[j] = mk ? mask_mul(v[j], mk[ml], mk[M + ml]) : v[j];
         }
       } else {  // gather at this CTA's interface pixels through the free exchange buffer
         cf* buf = phase ? b1 : b0;
@@ -280,25 +281,11 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   const int t = threadIdx.x;
   const int c = static_cast<int>(cl.block_rank());
   // global layout: M − 1 stage twiddles, then w_N^{c·k1} at (M − 1) + c·M + k1
-  const Tw<float>* xg = tw_global + (S::M - 1);
   const Tw<float>* tw = tw_global;
+  const Tw<float>* xg = tw_global + (S::M - 1);
   const Tw<float>* xf = xg + c * S::M;   // forward: this CTA's c, every k1
-  const Tw<float>* xi = nullptr;         // inverse: entry d·MB + k1l for k1 = c·MB + k1l
-  Tw<float>* xi_s = nullptr;
-  if constexpr (r2c::cluster_tw_in_smem<N, C>()) {
-    Tw<float>* tws = reinterpret_cast<Tw<float>*>(smem_raw + r2c::cluster_lines_bytes<N, C>());
-    Tw<float>* xfs = tws + (S::M - 1);
-    xi_s = xfs + S::M;
-    for (int i = t; i < S::M - 1; i += NT) tws[i] = tw_global[i];
-    for (int i = t; i < S::M; i += NT) xfs[i] = xf[i];
-    for (int i = t; i < S::M; i += NT) xi_s[i] = xg[(i / S::MB) * S::M + c * S::MB + i % S::MB];
-    __syncthreads();
-    tw = tws;
-    xf = xfs;
-    xi = xi_s;
-  } else {
-    xi = xg + c * S::MB;
-  }
+  const Tw<float>* xi = xg + c * S::MB;  // inverse: entry d·M + k1l for k1 = c·MB + k1l
+  float* mask_s = reinterpret_cast<float*>(smem_raw + r2c::cluster_lines_bytes<N, C>());
   int phase = 0, xphase = 0;
   for (;;) {
     if (c == 0 && t == 0) s_item = atomicAdd(queue, 1);
@@ -310,6 +297,15 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
     }
     const R2Item it = items[idx];
     if (c == 0 && t == 0) it.clock[0] = global_ns();
+    const float* mk = nullptr;
+    if (it.mask) {  // first read in the first step's epilogue, after the transforms' barriers
+      for (int m = t; m < S::M; m += NT) {
+        const int q = C * m + c;
+        mask_s[m] = it.mask[q];
+        mask_s[S::M + m] = it.mask[N + q];
+      }
+      mk = mask_s;
+    }
     cf v[E], out[E];
     const int iters = it.iterations > 0 ? it.iterations : 1;
 #pragma unroll
@@ -320,6 +316,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
       if (c == 0 && t == 0) it.energy[2 * iters] = pin;
     }
     const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
+    R2Next nx;
+    nx.st = it.steps[0];
+    nx.p0 = it.passes[nx.st.fwd_off];
     for (int sw = 0; sw < sweeps; ++sw) {
       const bool backward = sw & 1;
       const int iter = sw >> 1;
@@ -332,13 +331,17 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
       }
       for (int s = 0; s < it.nz; ++s) {
         const int p = backward ? it.nz - 1 - s : s;
-        const R2Step st = it.steps[p];
+        const R2Step st = nx.st;
+        const R2Pass p0 = nx.p0;
+        bool next_backward;
+        const int next_p = next_step(s, p, it.nz, sw, sweeps, backward, next_backward);
         const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, xb, xphase, it, st, backward, reflect,
-                                  store, add, tw, xf, xi, t, c, cl);
+        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, xb, xphase, it, st, p0, nx, next_p,
+                                  next_backward, backward, reflect, store, add, mk, tw, xf, xi, t,
+                                  c, cl);
       }
       cf* dst = backward ? it.reflected : it.transmitted;
 #pragma unroll

@@ -283,41 +283,74 @@ __device__ __forceinline__ double r2f_flux(const cf (&v)[N / NT], const double* 
   return total;
 }
 
-// The spectrum of a multi-pass step is kept in the shared line S at the owned positions (each
-// thread reads back only what it wrote, so S needs no barrier).
+// Bytes of `lines` padded lines of n points, rounded up to 16.
+__host__ __device__ constexpr std::size_t lines_bytes(int n, int lines) {
+  return (static_cast<std::size_t>(lines) * rf::padded(n) * sizeof(cf) + 15) / 16 * 16;
+}
+
+// Records of the next slab step, loaded while the current step computes: the step record first,
+// its first pass record once the step record has arrived (mid-step). Hides the chain of
+// dependent global loads (step record -> pass record -> table) behind the transforms.
+struct R2Next {
+  R2Step st;
+  R2Pass p0;
+};
+
+// The item's mask, (hi, lo) pairs, sits in shared memory beside the lines when it fits.
+template <int N>
+__host__ __device__ constexpr bool fixed_mask_in_smem() {
+  return lines_bytes(N, 3) + 2 * static_cast<std::size_t>(N) * sizeof(float) <= 220 * 1024;
+}
+template <int N>
+__host__ __device__ constexpr std::size_t fixed_smem_bytes() {
+  return lines_bytes(N, 3) + (fixed_mask_in_smem<N>() ? 2 * static_cast<std::size_t>(N) * sizeof(float) : 0);
+}
+
+// One slab step. st/p0: this step's record and first pass record (prefetched); nx receives the
+// records of step next_p (≥ 0) of direction next_backward. The spectrum of a multi-pass step is
+// kept in the shared line S at the owned positions (each thread reads back only what it wrote,
+// so S needs no barrier). mk: the item's mask (N hi values, then N lo values) or null.
 template <int N, int NT, class RADS>
 __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / NT],
                                          cf* b0, cf* b1, int& phase, const R2Item& it,
-                                         const R2Step& st, bool backward, bool reflect, cf* store,
-                                         const cf* add, const Tw<float>* __restrict__ tw, int t) {
+                                         const R2Step& st, const R2Pass& p0, R2Next& nx,
+                                         int next_p, bool next_backward, bool backward,
+                                         bool reflect, cf* store, const cf* add, const float* mk,
+                                         const Tw<float>* __restrict__ tw, int t) {
   constexpr int E = N / NT;
   const int off = backward ? st.bwd_off : st.fwd_off;
   const int ntp = backward ? st.bwd_t : st.fwd_t;
   const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
-  rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+  if (next_p >= 0) nx.st = it.steps[next_p];
   if (npass == 1) {  // one transmission pass over every pixel
-    const cf* m = it.tables + it.passes[off].tab;
+    // operator values first: their loads are in flight during the forward transform
+    const cf* m = it.tables + p0.tab;
+    cf th[E], tl[E];
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      const int q = t + k * NT;
-      v[k] = pmul(v[k], m[q], m[N + q]);
-      if ((k & 3) == 3) asm volatile("" ::: "memory");  // bound the loads in flight
+      th[k] = m[t + k * NT];
+      tl[k] = m[N + t + k * NT];
     }
+    rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+#pragma unroll
+    for (int k = 0; k < E; ++k) v[k] = pmul(v[k], th[k], tl[k]);
     rf::fft<+1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
-    if (it.mask)
+    if (mk)
 #pragma unroll
       for (int k = 0; k < E; ++k) {
         const int q = t + k * NT;
-        v[k] = mask_mul(v[k], it.mask[q], it.mask[N + q]);
-        if ((k & 3) == 3) asm volatile("" ::: "memory");
+        v[k] = mask_mul(v[k], mk[q], mk[N + q]);
       }
   } else {
+    rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
+    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
 #pragma unroll
     for (int k = 0; k < E; ++k) S[rf::pad(t + k * NT)] = v[k];
     for (int j = 0; j < npass; ++j) {
-      const R2Pass ps = it.passes[off + j];
+      const R2Pass ps = j == 0 ? p0 : it.passes[off + j];
       const cf* m = it.tables + ps.tab;
 #pragma unroll
       for (int k = 0; k < E; ++k) {
@@ -330,7 +363,7 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
 #pragma unroll
         for (int k = 0; k < E; ++k) {
           const int q = t + k * NT;
-          if (!pid || pid[q] == ps.pair) out[k] = it.mask ? mask_mul(v[k], it.mask[q], it.mask[N + q]) : v[k];
+          if (!pid || pid[q] == ps.pair) out[k] = mk ? mask_mul(v[k], mk[q], mk[N + q]) : v[k];
           if ((k & 3) == 3) asm volatile("" ::: "memory");
         }
       } else {  // gather at the interface pixels through the free exchange buffer
@@ -364,40 +397,32 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
   }
 }
 
-// Shared memory of a fixed-length kernel: three padded lines, then (16-byte aligned) the N − 1
-// stage twiddles of the class when they fit, loaded once per CTA; else they are read from
-// global memory (L2).
-__host__ __device__ constexpr std::size_t lines_bytes(int n, int lines) {
-  return (static_cast<std::size_t>(lines) * rf::padded(n) * sizeof(cf) + 15) / 16 * 16;
-}
-template <int N>
-__host__ __device__ constexpr bool fixed_tw_in_smem() {
-  return lines_bytes(N, 3) + static_cast<std::size_t>(N - 1) * sizeof(Tw<float>) <= 220 * 1024;
-}
-template <int N>
-__host__ __device__ constexpr std::size_t fixed_smem_bytes() {
-  return lines_bytes(N, 3) + (fixed_tw_in_smem<N>() ? static_cast<std::size_t>(N - 1) * sizeof(Tw<float>) : 0);
+// The step after step p of a sweep: the next one of the sweep, else the first of the next
+// sweep (−1: none).
+__device__ __forceinline__ int next_step(int s, int p, int nz, int sw, int sweeps, bool backward,
+                                         bool& next_backward) {
+  next_backward = backward;
+  if (s + 1 < nz) return backward ? p - 1 : p + 1;
+  if (sw + 1 < sweeps) {
+    next_backward = !backward;
+    return next_backward ? nz - 1 : 0;
+  }
+  return -1;
 }
 
 template <int N, int NT, class RADS>
 __global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __restrict__ items,
                                                          int nitems, int* queue,
-                                                         const Tw<float>* __restrict__ tw_global) {
+                                                         const Tw<float>* __restrict__ tw) {
   constexpr int E = N / NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cf* b0 = reinterpret_cast<cf*>(smem_raw);
   cf* b1 = b0 + rf::padded(N);
   cf* S = b1 + rf::padded(N);
+  float* mask_s = reinterpret_cast<float*>(smem_raw + lines_bytes(N, 3));
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
   const int t = threadIdx.x;
-  const Tw<float>* tw = tw_global;
-  if constexpr (fixed_tw_in_smem<N>()) {
-    Tw<float>* tws = reinterpret_cast<Tw<float>*>(smem_raw + lines_bytes(N, 3));
-    for (int i = t; i < N - 1; i += NT) tws[i] = tw_global[i];
-    __syncthreads();
-    tw = tws;
-  }
   int phase = 0;
   for (;;) {
     if (t == 0) s_item = atomicAdd(queue, 1);
@@ -406,6 +431,13 @@ __global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __rest
     if (idx >= nitems) return;
     const R2Item it = items[idx];
     if (t == 0) it.clock[0] = global_ns();
+    const float* mk = it.mask;
+    if constexpr (fixed_mask_in_smem<N>()) {
+      if (mk) {  // first read in the first step's epilogue, after the transforms' barriers
+        for (int i = t; i < 2 * N; i += NT) mask_s[i] = it.mask[i];
+        mk = mask_s;
+      }
+    }
     cf v[E], out[E];
     const int iters = it.iterations > 0 ? it.iterations : 1;
     r2f_load<N, NT>(v, it.input, t);
@@ -416,6 +448,9 @@ __global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __rest
     }
     // sweeps alternate forward (even) and backward (odd); iterations = 0: one forward sweep
     const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
+    R2Next nx;
+    nx.st = it.steps[0];
+    nx.p0 = it.passes[nx.st.fwd_off];
     for (int sw = 0; sw < sweeps; ++sw) {
       const bool backward = sw & 1;
       const int iter = sw >> 1;
@@ -427,12 +462,16 @@ __global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __rest
       }
       for (int s = 0; s < it.nz; ++s) {
         const int p = backward ? it.nz - 1 - s : s;  // step p: planes p and p + 1
-        const R2Step st = it.steps[p];
+        const R2Step st = nx.st;
+        const R2Pass p0 = nx.p0;
+        bool next_backward;
+        const int next_p = next_step(s, p, it.nz, sw, sweeps, backward, next_backward);
         const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        r2f_step<N, NT, RADS>(v, S, out, b0, b1, phase, it, st, backward, reflect, store, add, tw, t);
+        r2f_step<N, NT, RADS>(v, S, out, b0, b1, phase, it, st, p0, nx, next_p, next_backward,
+                              backward, reflect, store, add, mk, tw, t);
       }
       r2f_store<N, NT>(backward ? it.reflected : it.transmitted, v, t);
       if (it.iterations == 0) break;

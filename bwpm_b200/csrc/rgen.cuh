@@ -112,12 +112,15 @@ __device__ __forceinline__ double flux(const cf (&v)[E], const double* w, double
   return total;
 }
 
-// One slab step (cf. r2f_step); every thread of the block calls it.
+// One slab step (cf. r2f_step: prefetched records and operator values; mk: the item's mask in
+// shared memory, n hi then n lo values, or null); every thread of the block calls it.
 template <int E>
 __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf* b1, int& phase,
-                                     const R2Item& it, const R2Step& st, bool backward,
-                                     bool reflect, cf* store, const cf* add, const FftPlan& plan,
-                                     const Tw<float>* __restrict__ tw, int t, int nt) {
+                                     const R2Item& it, const R2Step& st, const R2Pass& p0,
+                                     R2Next& nx, int next_p, bool next_backward, bool backward,
+                                     bool reflect, cf* store, const cf* add, const float* mk,
+                                     const FftPlan& plan, const Tw<float>* __restrict__ tw, int t,
+                                     int nt) {
   const int n = it.n, nthr = static_cast<int>(blockDim.x);
   const bool own = t < nt;
   const int off = backward ? st.bwd_off : st.fwd_off;
@@ -125,49 +128,77 @@ __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf
   const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
-  fft<-1, E>(v, b0, b1, phase, plan, tw, t, nt);
-  if (npass > 1 && own) {
-#pragma unroll
-    for (int k = 0; k < E; ++k) S[rf::pad(t + k * nt)] = v[k];
-  }
-  for (int j = 0; j < npass; ++j) {
-    const R2Pass ps = it.passes[off + j];
-    const cf* m = it.tables + ps.tab;
+  if (next_p >= 0) nx.st = it.steps[next_p];
+  if (npass == 1) {
+    const cf* m = it.tables + p0.tab;
+    cf th[E], tl[E];  // in flight during the forward transform
     if (own) {
 #pragma unroll
       for (int k = 0; k < E; ++k) {
-        const int q = t + k * nt;
-        v[k] = pmul(npass > 1 ? S[rf::pad(q)] : v[k], m[q], m[n + q]);
-        if ((k & 3) == 3) asm volatile("" ::: "memory");
+        th[k] = m[t + k * nt];
+        tl[k] = m[n + t + k * nt];
       }
     }
+    fft<-1, E>(v, b0, b1, phase, plan, tw, t, nt);
+    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (own) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) v[k] = pmul(v[k], th[k], tl[k]);
+    }
     fft<+1, E>(v, b0, b1, phase, plan, tw, t, nt);
-    if (!ps.refl) {
+    if (own && mk) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        const int q = t + k * nt;
+        v[k] = mask_mul(v[k], mk[q], mk[n + q]);
+      }
+    }
+  } else {
+    fft<-1, E>(v, b0, b1, phase, plan, tw, t, nt);
+    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (own) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) S[rf::pad(t + k * nt)] = v[k];
+    }
+    for (int j = 0; j < npass; ++j) {
+      const R2Pass ps = j == 0 ? p0 : it.passes[off + j];
+      const cf* m = it.tables + ps.tab;
       if (own) {
 #pragma unroll
         for (int k = 0; k < E; ++k) {
           const int q = t + k * nt;
-          if (!pid || pid[q] == ps.pair) out[k] = it.mask ? mask_mul(v[k], it.mask[q], it.mask[n + q]) : v[k];
+          v[k] = pmul(S[rf::pad(q)], m[q], m[n + q]);
           if ((k & 3) == 3) asm volatile("" ::: "memory");
         }
       }
-    } else {  // gather at the interface pixels through the free exchange buffer
-      cf* buf = phase ? b1 : b0;
-      if (own) {
+      fft<+1, E>(v, b0, b1, phase, plan, tw, t, nt);
+      if (!ps.refl) {
+        if (own) {
 #pragma unroll
-        for (int k = 0; k < E; ++k) buf[rf::pad(t + k * nt)] = v[k];
+          for (int k = 0; k < E; ++k) {
+            const int q = t + k * nt;
+            if (!pid || pid[q] == ps.pair) out[k] = mk ? mask_mul(v[k], mk[q], mk[n + q]) : v[k];
+            if ((k & 3) == 3) asm volatile("" ::: "memory");
+          }
+        }
+      } else {  // gather at the interface pixels through the free exchange buffer
+        cf* buf = phase ? b1 : b0;
+        if (own) {
+#pragma unroll
+          for (int k = 0; k < E; ++k) buf[rf::pad(t + k * nt)] = v[k];
+        }
+        __syncthreads();
+        for (int k = t; k < st.niface; k += nthr) {
+          const int q = iface[k];
+          if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q)];
+        }
+        phase ^= 1;
       }
-      __syncthreads();
-      for (int k = t; k < st.niface; k += nthr) {
-        const int q = iface[k];
-        if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q)];
-      }
-      phase ^= 1;
     }
-  }
-  if (own) {
+    if (own) {
 #pragma unroll
-    for (int k = 0; k < E; ++k) v[k] = out[k];
+      for (int k = 0; k < E; ++k) v[k] = out[k];
+    }
   }
   if (add) {  // sparse sources of the other pass at this step's interface pixels
     cf* buf = phase ? b1 : b0;
@@ -194,10 +225,11 @@ __host__ __device__ constexpr int rt_max_threads(int e) { return e <= 8 ? 512 : 
 
 }  // namespace rg
 
-// Shared memory of the run-time-length kernel for lines up to n points: three padded lines and
-// the stage twiddles of the item in progress.
+// Shared memory of the run-time-length kernel for lines up to n points: three padded lines, the
+// stage twiddles and the mask of the item in progress.
 __host__ __device__ constexpr std::size_t rt_smem_bytes(int n) {
-  return lines_bytes(n, 3) + static_cast<std::size_t>(n - 1) * sizeof(Tw<float>);
+  return lines_bytes(n, 3) + static_cast<std::size_t>(n - 1) * sizeof(Tw<float>) +
+         2 * static_cast<std::size_t>(n) * sizeof(float);  // + the mask
 }
 
 // Persistent kernel over items of any length n = E·nt (nt ≤ blockDim, plan per item).
@@ -226,6 +258,12 @@ __global__ void __launch_bounds__(rg::rt_max_threads(E), 1)
       it.clock[0] = global_ns();
     }
     for (int i = t; i < n - 1; i += static_cast<int>(blockDim.x)) tws[i] = sh.twiddles[base + i];
+    float* mask_s = reinterpret_cast<float*>(tws + (n - 1));
+    const float* mk = nullptr;
+    if (it.mask) {
+      for (int i = t; i < 2 * n; i += static_cast<int>(blockDim.x)) mask_s[i] = it.mask[i];
+      mk = mask_s;
+    }
     __syncthreads();
     const FftPlan& plan = s_plan;
     cf* b0 = reinterpret_cast<cf*>(smem_raw);
@@ -244,6 +282,9 @@ __global__ void __launch_bounds__(rg::rt_max_threads(E), 1)
       if (t == 0) it.energy[2 * iters] = pin;
     }
     const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
+    R2Next nx;
+    nx.st = it.steps[0];
+    nx.p0 = it.passes[nx.st.fwd_off];
     for (int sw = 0; sw < sweeps; ++sw) {
       const bool backward = sw & 1;
       const int iter = sw >> 1;
@@ -253,12 +294,16 @@ __global__ void __launch_bounds__(rg::rt_max_threads(E), 1)
       }
       for (int s = 0; s < it.nz; ++s) {
         const int p = backward ? it.nz - 1 - s : s;
-        const R2Step st = it.steps[p];
+        const R2Step st = nx.st;
+        const R2Pass p0 = nx.p0;
+        bool next_backward;
+        const int next_p = next_step(s, p, it.nz, sw, sweeps, backward, next_backward);
         const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        rg::step<E>(v, S, out, b0, b1, phase, it, st, backward, reflect, store, add, plan, tws, t, nt);
+        rg::step<E>(v, S, out, b0, b1, phase, it, st, p0, nx, next_p, next_backward, backward,
+                    reflect, store, add, mk, plan, tws, t, nt);
       }
       cf* dst = backward ? it.reflected : it.transmitted;
       if (own) {
