@@ -231,7 +231,12 @@ def run_ours(args) -> None:
     params = _params()
     t_setup = time.perf_counter()
     b = Batch2D(device)
-    b.set_autotune(True)  # kernel variant per length chosen by measurement at prepare
+    if args.variants:  # profiling: the kernel choice of an earlier (timed) run, no autotuning
+        for spec in args.variants.split(","):
+            ny, v = spec.split(":")
+            b.set_variant(int(ny), int(v))
+    else:
+        b.set_autotune(True)  # kernel variant per length chosen by measurement at prepare
     fields = []
     for prm in params:
         p = workloads.tilted_slab2d_from(prm)
@@ -433,6 +438,8 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--served-fp64", type=int, default=3, help="FP64 sample of the served stream")
+    ap.add_argument("--variants", type=str, default="",
+                    help="profiling only: NY:VARIANT,... forces kernel variants (no autotuning)")
     ap.add_argument("--reduced", type=str, default="",
                     help="profiling only: COUNT,NZ_MAX,ITERATIONS[,NY] (first COUNT solves, chains "
                          "capped, optionally all of length NY); skips the FP64, served and CPU "

@@ -981,7 +981,7 @@ void Batch2DImpl::autotune() {
         const Meas t = measure();
         // clearly faster batch, or an equal batch (within the run-to-run spread) whose class
         // needs clearly less SM time (frees SMs for the other classes)
-        const bool faster = t.ms < 0.985f * current.ms;
+        const bool faster = t.ms < 0.98f * current.ms;
         const bool leaner = t.ms < 1.01f * current.ms && t.class_sm[c] < 0.8 * current.class_sm[c];
         if (faster || leaner) {
           current = t;

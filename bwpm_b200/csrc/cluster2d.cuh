@@ -9,7 +9,8 @@
 //   inverse:  Z_c[k1] = Σ_k2 X[k1 + M·k2]·w_C^{−c·k2}·w_N^{−c·k1};  exchange;
 //             x_c = IDFT_M(Z_c)
 // (a two-factor Cooley-Tukey split, N = M·C), each exchange one all-to-all through distributed
-// shared memory between two cluster barriers' worth of work. The local M-point transforms are
+// shared memory: every CTA stores its values straight into the owners' buffers (remote stores
+// need no round trip), one cluster barrier, then local reads. The local M-point transforms are
 // the register-resident transforms of rfft.cuh. Exchange buffers alternate, so one cluster
 // barrier per exchange suffices: a buffer is written again only after a later exchange's
 // barrier, which every CTA reaches after its reads of the earlier one.
@@ -73,18 +74,21 @@ __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
   using S = Shape<N, C, NT>;
   rf::fft<-1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
   cf* x = xb[xphase];
+  // push: Y_c[k1]·w_N^{c·k1} goes to the owner of k1's block (CTA j / EB, since
+  // k1 = t + j·NT = (j / EB)·MB + (j mod EB)·NT + t), slot c·MB + (k1 mod MB) of its buffer
 #pragma unroll
   for (int j = 0; j < S::E; ++j) {
     const int k1 = t + j * NT;
-    x[k1] = c == 0 ? v[j] : twmul<-1>(v[j], xf[k1]);
+    cf* dst = cl.map_shared_rank(x, j / S::EB);
+    dst[c * S::MB + (j % S::EB) * NT + t] = c == 0 ? v[j] : twmul<-1>(v[j], xf[k1]);
   }
   cl.sync();
 #pragma unroll
   for (int i = 0; i < S::EB; ++i) {
-    const int k1 = c * S::MB + i * NT + t;
+    const int k1l = i * NT + t;
     cf u[C];
 #pragma unroll
-    for (int r = 0; r < C; ++r) u[r] = cl.map_shared_rank(x, r)[k1];
+    for (int r = 0; r < C; ++r) u[r] = x[r * S::MB + k1l];
     rf::dft<-1, C>(u);
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) v[k2 * S::EB + i] = u[k2];
@@ -107,17 +111,17 @@ __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) u[k2] = v[k2 * S::EB + i];
     rf::dft<+1, C>(u);
-    // inverse cross twiddle w_N^{−d·k1}, k1 = c·MB + k1l: entry d·M + k1l of xi = table + c·MB
+    // push Z_d[k1]·w_N^{−d·k1} (k1 = c·MB + k1l; the twiddle is entry d·M + k1l of
+    // xi = table + c·MB) to CTA d, slot k1 of its buffer
 #pragma unroll
-    for (int d = 0; d < C; ++d) x[d * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xi[d * S::M + k1l]);
+    for (int d = 0; d < C; ++d) {
+      cf* dst = cl.map_shared_rank(x, d);
+      dst[c * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xi[d * S::M + k1l]);
+    }
   }
   cl.sync();
 #pragma unroll
-  for (int j = 0; j < S::E; ++j) {
-    // k1 = t + j·NT lies in the block of CTA j / EB, at local index (j mod EB)·NT + t
-    const cf* src = cl.map_shared_rank(x, j / S::EB);
-    v[j] = src[c * S::MB + (j % S::EB) * NT + t];
-  }
+  for (int j = 0; j < S::E; ++j) v[j] = x[t + j * NT];
   xphase ^= 1;
   rf::fft<+1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
 }

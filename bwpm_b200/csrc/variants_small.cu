@@ -14,15 +14,14 @@ FixedVariant fixed() {
 }  // namespace
 
 void add_variants_small(std::vector<FixedVariant>& v) {
+  // per length, only variants that no other variant beats in both per-step latency and SM time
+  // (measured on a B200: 1 item, tilted slab, 400 slabs)
   v.push_back(fixed<256, 32, 8, 8, 4>());
   v.push_back(fixed<384, 32, 4, 4, 4, 3, 2>());
   v.push_back(fixed<512, 64, 8, 8, 8>());
-  v.push_back(fixed<512, 32, 16, 8, 4>());
   v.push_back(fixed<768, 64, 4, 4, 4, 4, 3>());
   v.push_back(fixed<1024, 128, 8, 8, 8, 2>());
-  v.push_back(fixed<1024, 64, 16, 16, 4>());
   v.push_back(fixed<1536, 128, 4, 4, 4, 4, 2, 3>());
-  v.push_back(fixed<1536, 64, 8, 8, 8, 3>());
 }
 
 const std::vector<FixedVariant>& fixed_variants() {

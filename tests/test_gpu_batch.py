@@ -186,16 +186,16 @@ def test_every_kernel_variant_matches_fp64(n):
 def test_autotuned_batch_equals_forced_variant():
     """Autotuning picks a variant per length; the results equal a run forced to that variant."""
     from bwpm_b200 import workloads
-    from bwpm_b200.batch import Batch2D
+    from bwpm_b200.batch import Batch2D, variant_count
 
-    probs = workloads.batch2d(count=8, seed=31, sizes=(512, 1536, 3072), nz_range=(30, 60),
+    probs = workloads.batch2d(count=8, seed=31, sizes=(1024, 4096, 6144, 8192), nz_range=(30, 60),
                               iterations=2)
     b = Batch2D()
     b.set_autotune(True)
     ids = [b.add_problem(p) for p in probs]
     b.run()
     cls = {c["ny"]: c for c in b.classes()}
-    assert all(c["tuned_ms"] > 0 for c in cls.values())
+    assert all((c["tuned_ms"] > 0) == (variant_count(n) > 1) for n, c in cls.items())
     forced = Batch2D()
     for n, c in cls.items():
         forced.set_variant(n, c["variant"])
