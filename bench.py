@@ -437,7 +437,7 @@ def main() -> None:
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="target CPU seconds per core")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
-    ap.add_argument("--served-fp64", type=int, default=3, help="FP64 sample of the served stream")
+    ap.add_argument("--served-fp64", type=int, default=6, help="FP64 sample of the served stream")
     ap.add_argument("--variants", type=str, default="",
                     help="profiling only: NY:VARIANT,... forces kernel variants (no autotuning)")
     ap.add_argument("--reduced", type=str, default="",

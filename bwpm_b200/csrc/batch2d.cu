@@ -56,35 +56,56 @@ int fixed_length_index(int n) {
   return it != l.end() && *it == n ? static_cast<int>(it - l.begin()) : -1;
 }
 
-// Radices (largest first) of a length n for a run-time-length kernel with E values per thread:
-// each radix divides E; empty if n has another prime factor or E lacks one of n's.
+// Radices of a length n for a run-time-length kernel with E values per thread: the powers of two
+// as 8s (4s, 2s) when E allows, then 3s and 5s; empty if n has another prime factor. Stages
+// whose radix does not divide E run as gather stages (rgen.cuh).
 std::vector<int> rt_radices(int n, int e) {
   std::vector<int> r;
-  int m = n;
-  for (int p : {8, 4, 2, 5, 3}) {
-    if (e % p) continue;
+  int m = n, twos = 0;
+  while (m % 2 == 0) {
+    m /= 2;
+    ++twos;
+  }
+  const int big = e % 8 == 0 ? 8 : e % 4 == 0 ? 4 : e % 2 == 0 ? 2 : 4;
+  const int lb = big == 8 ? 3 : big == 4 ? 2 : 1;
+  while (twos >= lb) {
+    r.push_back(big);
+    twos -= lb;
+  }
+  if (twos == 2) r.push_back(4);
+  if (twos == 1) r.push_back(2);
+  for (int p : {3, 5})
     while (m % p == 0) {
       r.push_back(p);
       m /= p;
     }
-  }
   if (m != 1) return {};
-  std::stable_sort(r.begin(), r.end(), [](int a, int b) { return a > b; });
   return r;
 }
 
-// Position in rt_variants() of the run-time-length kernel for length n: the smallest E (the most
-// threads) whose radices factor n, within the kernel's thread limit and the shared memory of
-// three padded lines; −1 if none.
+// Position in rt_variants() of the run-time-length kernel for length n, or −1: among the E
+// that divide n within the kernel's thread limit, the smallest estimated per-thread work over
+// the stages (measured: more threads with fewer values each beat fewer stages).
 int rt_choice(int n) {
   const auto& rv = rt_variants();
   if (rt_smem_bytes(n) > 220 * 1024) return -1;
+  int best = -1;
+  double best_score = 1e30;
   for (std::size_t i = 0; i < rv.size(); ++i) {
     const int e = rv[i].e;
-    if (n % e || n / e > rg::rt_max_threads(e) || rt_radices(n, e).empty()) continue;
-    return static_cast<int>(i);
+    if (n % e || n / e > rg::rt_max_threads(e)) continue;
+    const std::vector<int> r = rt_radices(n, e);
+    if (r.empty()) continue;
+    // a stage costs about (8 + E) value-times per thread (E values plus fixed overhead), twice
+    // for a gather stage
+    double score = 0;
+    for (int x : r) score += (e % x == 0 ? 1.0 : 2.0) * (8.0 + e);
+    if (score < best_score - 1e-9) {
+      best_score = score;
+      best = static_cast<int>(i);
+    }
   }
-  return -1;
+  return best;
 }
 
 // indices into fixed_variants() of the variants of length n (first: the default)

@@ -66,6 +66,9 @@ class PlaneSolver final : public Solver {
   void born_sources(const C* spec, int slot, int dir);
   void born_emission(int slot, int dir, C* plane);
   void gmres(int slot, int dir);
+  // the forward/backward sweeps of a run (device work only, unless Born slabs need GMRES)
+  void sweeps(int iterations, const std::vector<int>& keep_slot, DevBuf<C>& kept_f, DevBuf<C>& kept_b,
+              DevBuf<C>& t_iter, DevBuf<C>& r_iter);
   cd dot(const C* u, const C* v, long long m);
   void axpby(C* y, const C* x, cd a, cd b, long long m);
   void add_plane_scaled(C* dst, const C* src, const T* mask);
@@ -100,6 +103,7 @@ class PlaneSolver final : public Solver {
   // fields
   DevBuf<C> input_, e_, next_, spec_, xbuf_, work_, src_fwd_, src_bwd_;
   DevBuf<cd> stage_;
+  C* last_e_ = nullptr;  // plane holding the last sweep's result (set by sweeps)
   int max_pass_ = 1;
   // Born
   std::vector<cd> hosts_;
@@ -637,25 +641,12 @@ void PlaneSolver<T>::born_emission(int slot, int dir, C* plane) {
 }
 
 template <typename T>
-void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* keep,
-                         std::size_t nkeep, RunOutputs& out) {
-  check_cuda(cudaSetDevice(in_.device), "cudaSetDevice");
+void PlaneSolver<T>::sweeps(int iterations, const std::vector<int>& keep_slot, DevBuf<C>& kept_f,
+                            DevBuf<C>& kept_b, DevBuf<C>& t_iter, DevBuf<C>& r_iter) {
   const std::size_t nn = n();
   const long long n2 = 2 * static_cast<long long>(nn);
   const int nz = static_cast<int>(in_.nz);
   const int iters = std::max(iterations, 1);
-  // keep planes: device slots
-  std::vector<int> keep_slot(nz + 1, -1);
-  for (std::size_t i = 0; i < nkeep; ++i)
-    if (keep[i] >= 0 && keep[i] <= nz) keep_slot[keep[i]] = static_cast<int>(i);
-  DevBuf<C> kept_f(nkeep * 2 * nn, stream_), kept_b(nkeep * 2 * nn, stream_), t_iter, r_iter;
-  if (iterations > 0) {
-    t_iter.alloc(iterations * 2 * nn, stream_);
-    r_iter.alloc(iterations * 2 * nn, stream_);
-  }
-  check_cuda(cudaMemcpyAsync(stage_.ptr, field, n2 * sizeof(cd), cudaMemcpyHostToDevice, stream_), "field upload");
-  launch(k_convert<T, double>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, input_.ptr,
-         (const cd*)stage_.ptr, n2);
   auto copy = [&](C* dst, const C* src) {
     check_cuda(cudaMemcpyAsync(dst, src, n2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
   };
@@ -709,6 +700,31 @@ void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* ke
     }
     copy(r_iter.ptr + it * n2, e);
   }
+  last_e_ = e;
+}
+
+template <typename T>
+void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* keep,
+                         std::size_t nkeep, RunOutputs& out) {
+  check_cuda(cudaSetDevice(in_.device), "cudaSetDevice");
+  const std::size_t nn = n();
+  const long long n2 = 2 * static_cast<long long>(nn);
+  const int nz = static_cast<int>(in_.nz);
+  const int iters = std::max(iterations, 1);
+  // keep planes: device slots
+  std::vector<int> keep_slot(nz + 1, -1);
+  for (std::size_t i = 0; i < nkeep; ++i)
+    if (keep[i] >= 0 && keep[i] <= nz) keep_slot[keep[i]] = static_cast<int>(i);
+  DevBuf<C> kept_f(nkeep * 2 * nn, stream_), kept_b(nkeep * 2 * nn, stream_), t_iter, r_iter;
+  if (iterations > 0) {
+    t_iter.alloc(iterations * 2 * nn, stream_);
+    r_iter.alloc(iterations * 2 * nn, stream_);
+  }
+  check_cuda(cudaMemcpyAsync(stage_.ptr, field, n2 * sizeof(cd), cudaMemcpyHostToDevice, stream_), "field upload");
+  launch(k_convert<T, double>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, input_.ptr,
+         (const cd*)stage_.ptr, n2);
+  sweeps(iterations, keep_slot, kept_f, kept_b, t_iter, r_iter);
+  C* e = last_e_;
   // outputs
   auto download = [&](const C* src, cd* dst) {
     if (!dst) return;

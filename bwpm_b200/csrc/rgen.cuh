@@ -2,10 +2,11 @@
 //
 // The fixed-length kernels (rfft.cuh, k_resident2d_fixed) unroll everything for one N. This
 // variant keeps the number of values per thread E a compile-time constant and takes the line
-// length n = E·nt (nt ≤ blockDim threads own values) and the radix order at run time, so one
-// kernel serves every length whose radices all divide E (E = 15 serves 3^a·5^b, E = 12 serves
-// 2^a·3^b, E = 20 serves 2^a·5^b, …). Each stage is the owned-pattern Stockham stage of rfft.cuh
-// with a compile-time radix chosen by a switch; the run-time sub-length L costs one integer
+// length n = E·nt (nt ≤ blockDim threads own values) and the radix order (2, 3, 4, 5, 8) at
+// run time, so one kernel serves many lengths. A stage whose radix divides E is the
+// owned-pattern Stockham stage of rfft.cuh (one exchange); any other stage gathers whole
+// butterflies from shared memory (two exchanges), so E need not contain every prime of n (the
+// host picks E and the radix order per length). The run-time sub-length L costs one integer
 // modulo per butterfly. Items of different lengths share a launch: threads t ≥ nt of an item
 // own no values and only join the barriers.
 #pragma once
@@ -53,35 +54,69 @@ __device__ __forceinline__ void stage(cf (&v)[E], cf* buf, const Tw<float>* __re
   }
 }
 
+// A stage whose radix does not divide E: the owned values go to shared memory, each thread
+// gathers whole butterflies (i = t + j·nt < n/R, a run-time count), writes the outputs to the
+// other buffer, and reads back its owned values. Two barriers instead of one; `phase` is left
+// as it was (both buffers were used, the last reads were from the other one).
+template <int DIR, int E, int R>
+__device__ __forceinline__ void stage_gather(cf (&v)[E], cf* in_buf, cf* out_buf,
+                                             const Tw<float>* __restrict__ tw, int t, int nt, int n,
+                                             int L, int off) {
+  if (t < nt) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) in_buf[rf::pad(t + m * nt)] = v[m];
+  }
+  __syncthreads();
+  const int nb = n / R;
+  for (int i = t; i < nb; i += nt) {
+    const int k = i % L;
+    cf u[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) u[r] = in_buf[rf::pad(i + r * nb)];
+    if (L > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) u[r] = twmul<DIR>(u[r], tw[off + (r - 1) * L + k]);
+    }
+    rf::dft<DIR, R>(u);
+    const int base = (i - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out_buf[rf::pad(base + r * L)] = u[r];
+  }
+  __syncthreads();
+  if (t < nt) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = out_buf[rf::pad(t + m * nt)];
+  }
+}
+
 // In-register transform (DIR −1 forward, +1 inverse unnormalised) of a line of E·nt points with
 // the stages of `plan`; `phase` as in rf::fft. Every thread of the block must call it.
+template <int DIR, int E, int R>
+__device__ __forceinline__ void any_stage(cf (&v)[E], cf* b0, cf* b1, int& phase,
+                                          const Tw<float>* __restrict__ tw, int t, int nt, int n,
+                                          int L, int off, bool last) {
+  if constexpr (E % R == 0) {
+    stage<DIR, E, R>(v, phase ? b1 : b0, tw, t, nt, L, off, last);
+    if (!last) phase ^= 1;
+  } else {
+    stage_gather<DIR, E, R>(v, phase ? b1 : b0, phase ? b0 : b1, tw, t, nt, n, L, off);
+  }
+}
+
 template <int DIR, int E>
 __device__ __forceinline__ void fft(cf (&v)[E], cf* b0, cf* b1, int& phase, const FftPlan& plan,
                                    const Tw<float>* __restrict__ tw, int t, int nt) {
   for (int s = 0; s < plan.nstages; ++s) {
     const bool last = s == plan.nstages - 1;
-    cf* buf = phase ? b1 : b0;
     const int L = plan.len[s], off = plan.twoff[s];
     switch (plan.radix[s]) {
-      case 2:
-        if constexpr (E % 2 == 0) stage<DIR, E, 2>(v, buf, tw, t, nt, L, off, last);
-        break;
-      case 3:
-        if constexpr (E % 3 == 0) stage<DIR, E, 3>(v, buf, tw, t, nt, L, off, last);
-        break;
-      case 4:
-        if constexpr (E % 4 == 0) stage<DIR, E, 4>(v, buf, tw, t, nt, L, off, last);
-        break;
-      case 5:
-        if constexpr (E % 5 == 0) stage<DIR, E, 5>(v, buf, tw, t, nt, L, off, last);
-        break;
-      case 8:
-        if constexpr (E % 8 == 0) stage<DIR, E, 8>(v, buf, tw, t, nt, L, off, last);
-        break;
-      default:
-        break;  // the host plans only radices that divide E
+      case 2: any_stage<DIR, E, 2>(v, b0, b1, phase, tw, t, nt, plan.n, L, off, last); break;
+      case 3: any_stage<DIR, E, 3>(v, b0, b1, phase, tw, t, nt, plan.n, L, off, last); break;
+      case 4: any_stage<DIR, E, 4>(v, b0, b1, phase, tw, t, nt, plan.n, L, off, last); break;
+      case 5: any_stage<DIR, E, 5>(v, b0, b1, phase, tw, t, nt, plan.n, L, off, last); break;
+      case 8: any_stage<DIR, E, 8>(v, b0, b1, phase, tw, t, nt, plan.n, L, off, last); break;
+      default: break;  // the host plans radices 2, 3, 4, 5 and 8 only
     }
-    if (!last) phase ^= 1;
   }
 }
 
