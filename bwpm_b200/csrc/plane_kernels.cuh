@@ -220,6 +220,8 @@ struct RowSelect {
   const int* rowoff;        // (ny + 1) offsets into iface per row
   cx<T>* refl_out;          // (niface, 2) or null
   const cx<T>* add;         // (niface, 2) or null
+  cx<T>* xnext;             // or null: also the x transform of the output rows (the next step's
+                            // first transform, fused here)
   int ny, nx, rows;
   T inv_n;
 };
@@ -276,6 +278,22 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, S
       a.out[2 * q] = a.out[2 * q] + a.add[2 * k];
       a.out[2 * q + 1] = a.out[2 * q + 1] + a.add[2 * k + 1];
     }
+  if (a.xnext) {  // forward x transform of this CTA's output rows (written by this CTA above)
+    __syncthreads();
+    for (int idx = tid; idx < total; idx += nt) {
+      const int row = idx / per_row, rem = idx - row * per_row;
+      const int x = rem >> 1, c = rem & 1;
+      buf[(x * rows + row) * 2 + c] =
+          row < here ? a.out[(static_cast<long long>(y0 + row) * nx + x) * 2 + c] : cx<T>{0, 0};
+    }
+    __syncthreads();
+    fft_smem<-1>(buf, plan, tw, 2 * rows, tid, nt);
+    for (int idx = tid; idx < here * per_row; idx += nt) {
+      const int row = idx / per_row, rem = idx - row * per_row;
+      const int x = rem >> 1, c = rem & 1;
+      a.xnext[(static_cast<long long>(y0 + row) * nx + x) * 2 + c] = buf[(x * rows + row) * 2 + c];
+    }
+  }
 }
 
 // ---- small helpers ------------------------------------------------------------------------

@@ -58,8 +58,10 @@ class PlaneSolver final : public Solver {
   void setup();
   const C* table(int kind, cd nr, cd ns);
   StepPasses passes(int step, bool backward, bool reflect);
+  // x_ready: xbuf_ already holds the x transform of `in` (3D, fused into the previous step);
+  // x_next: also leave the x transform of `out` in xbuf_ for the next step
   void step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out, const C* add,
-            bool want_spec);
+            bool want_spec, bool x_ready = false, bool x_next = false);
   void fft_plane(const C* in, C* out, int ncomp, int dir);
   void born_operator(const C* in, C* out, int slot, int dir);
   void born_step(const C* spec, C* inc, int slot, int dir);
@@ -399,7 +401,7 @@ StepPasses PlaneSolver<T>::passes(int s, bool backward, bool reflect) {
 
 template <typename T>
 void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out,
-                          const C* add, bool want_spec) {
+                          const C* add, bool want_spec, bool x_ready, bool x_next) {
   const StepInfo& st = steps_[s];
   const StepPasses ps = passes(s, backward, reflect);
   const std::uint8_t* pid = st.pid_off >= 0 ? pid_pool_.ptr + st.pid_off : nullptr;
@@ -424,8 +426,9 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
     return;
   }
   const int ny = static_cast<int>(in_.ny), nx = static_cast<int>(in_.nx);
-  launch(k_rows_fft<-1, T>, dim3(ceil_div(ny, rows2_.rows)), dim3(rows2_.threads), rows2_.smem, in,
-         xbuf_.ptr, ny, nx, 2, rows2_.rows, hx_.plan, tw_x_.ptr);
+  if (!x_ready)
+    launch(k_rows_fft<-1, T>, dim3(ceil_div(ny, rows2_.rows)), dim3(rows2_.threads), rows2_.smem, in,
+           xbuf_.ptr, ny, nx, 2, rows2_.rows, hx_.plan, tw_x_.ptr);
   const LaunchShape& cs = ps.npass > 1 ? cols2_ : cols1_;
   ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cs.rows};
   launch(k_cols_step<T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem, c, ps, hy_.plan,
@@ -439,6 +442,7 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   r.rowoff = st.rowoff_off >= 0 ? rowoff_pool_.ptr + st.rowoff_off : nullptr;
   r.refl_out = refl_out;
   r.add = add;
+  r.xnext = x_next ? xbuf_.ptr : nullptr;
   r.ny = ny;
   r.nx = nx;
   r.rows = sel_.rows;
@@ -662,7 +666,11 @@ void PlaneSolver<T>::sweeps(int iterations, const std::vector<int>& keep_slot, D
       const bool reflect = iterations > 0 && st.niface > 0;
       const C* add = (it > 0 && st.niface > 0) ? src_fwd_.ptr + 2 * st.iface_off : nullptr;
       const bool host = born && st.host_slot >= 0;
-      step(p, false, reflect, e, next, reflect ? src_bwd_.ptr + 2 * st.iface_off : nullptr, add, host);
+      // 3D without Born slabs: each step leaves the next one's x transform (nothing else
+      // touches the plane between two steps of a sweep)
+      const bool fuse = !is2d() && !born;
+      step(p, false, reflect, e, next, reflect ? src_bwd_.ptr + 2 * st.iface_off : nullptr, add, host,
+           fuse && p > 0, fuse && p + 1 < nz);
       if (host) {
         born_step(spec_.ptr, inc_.ptr, st.host_slot, +1);
         add_plane_scaled(next, inc_.ptr, mask_.ptr);
@@ -692,7 +700,9 @@ void PlaneSolver<T>::sweeps(int iterations, const std::vector<int>& keep_slot, D
       }
       const bool reflect = st.niface > 0;
       const C* add = st.niface > 0 ? src_bwd_.ptr + 2 * st.iface_off : nullptr;
-      step(p - 1, true, reflect, e, next, reflect ? src_fwd_.ptr + 2 * st.iface_off : nullptr, add, false);
+      const bool fuse = !is2d() && !born;
+      step(p - 1, true, reflect, e, next, reflect ? src_fwd_.ptr + 2 * st.iface_off : nullptr, add, false,
+           fuse && p < nz, fuse && p > 1);
       std::swap(e, next);
       if (born && p >= 2 && steps_[p - 2].host_slot >= 0)
         add_plane_scaled(e, born_bwd_.ptr + steps_[p - 2].host_slot * n2, nullptr);  // born_bwd[p − 1]
