@@ -42,35 +42,22 @@ FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs × FP32 lanes × FMA
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    if ws <= 1:
-        return None, 0, 1
-    import torch
-    import torch.distributed as dist
+    from bwpm_b200 import replicas
 
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    from datetime import timedelta
-
-    dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                            device_id=torch.device("cuda", local))
+    dist, rank, ws, _ = replicas.init("nccl")
     return dist, rank, ws
 
 
 def _max_over_ranks(dist, x: float) -> float:
-    if dist is None:
-        return x
-    import torch
+    from bwpm_b200 import replicas
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(dist, x)
 
 
 def _barrier(dist):
-    if dist is not None:
-        dist.barrier()
+    from bwpm_b200 import replicas
+
+    replicas.barrier(dist)
 
 
 class Clocks:
@@ -224,7 +211,7 @@ def _params():
 def run_ours(args) -> None:
     dist, rank, ws = _dist()
     device = int(os.environ.get("LOCAL_RANK", "0")) if dist else 0
-    from bwpm_b200 import _core, workloads
+    from bwpm_b200 import _core, replicas, workloads
     from bwpm_b200.batch import Batch2D, flush_l2, host_register, host_unregister
     from bwpm_b200.model import Grid2D, power_flux
 
@@ -277,7 +264,7 @@ def run_ours(args) -> None:
     if rank != 0:
         _barrier(dist)
         return
-    value = ws * count / (step_ms * 1e-3)
+    value = replicas.throughput(ws, count, step_ms)
     # plain per-solve FP64 GPU path (drop-in CudaSolver) on a seeded sample; L2 error of the
     # batched complex64 results against it
     rng = np.random.default_rng(7)
