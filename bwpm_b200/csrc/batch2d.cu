@@ -352,6 +352,7 @@ class Batch2DImpl final : public Batch2D {
   void download();
   void use_variant(int c, int v);
   void autotune();
+  void check_status();
   // a compiled fixed-length kernel serves n (unless the run-time-length kernel was forced)
   bool uses_fixed(int n) const {
     auto f = forced_.find(n);
@@ -399,6 +400,7 @@ class Batch2DImpl final : public Batch2D {
   DevBuf<float> d_mask_;
   DevBuf<double> d_weights_, d_energy_;
   DevBuf<long long> d_clock_;
+  DevBuf<int> d_status_;
   DevBuf<R2Item> d_items_;
   DevBuf<int> d_queue_;
   DevBuf<ItemIo> d_io_;
@@ -718,6 +720,8 @@ void Batch2DImpl::prepare() {
   d_weights_.alloc(nweights, main_);
   d_energy_.alloc(nenergy, main_);
   d_clock_.alloc(2 * items_.size(), main_);
+  d_status_.alloc(1, main_);
+  d_status_.zero();
   d_items_.alloc(items_.size(), main_);
   d_queue_.alloc(kNumClasses, main_);
   d_io_.alloc(items_.size(), main_);
@@ -768,6 +772,7 @@ void Batch2DImpl::prepare() {
     item_energy_off_[k] = eoff;
     eoff += 2LL * std::max(1, h.in.iterations) + 1;
     r.clock = d_clock_.ptr + 2 * k;
+    r.status = d_status_.ptr;
     r.n = n;
     r.nz = h.in.nz;
     r.iterations = h.in.iterations;
@@ -1063,6 +1068,15 @@ bool Batch2DImpl::ready() {
   return true;
 }
 
+// A bounded wait inside a kernel gave up (a cluster exchange that never completed): the results
+// of that run are not valid.
+void Batch2DImpl::check_status() {
+  int st = 0;
+  check_cuda(cudaMemcpyAsync(&st, d_status_.ptr, sizeof(int), cudaMemcpyDeviceToHost, main_), "status");
+  check_cuda(cudaStreamSynchronize(main_), "status");
+  if (st != 0) throw std::runtime_error("resident 2D engine: a cluster exchange timed out");
+}
+
 float Batch2DImpl::run() {
   if (!prepared_) prepare();
   check_cuda(cudaSetDevice(device_), "cudaSetDevice");
@@ -1072,6 +1086,7 @@ float Batch2DImpl::run() {
   check_cuda(cudaEventSynchronize(ev_stop_), "run");
   float ms = 0;
   check_cuda(cudaEventElapsedTime(&ms, ev_start_, ev_stop_), "elapsed");
+  check_status();
   return ms;
 }
 
@@ -1098,6 +1113,7 @@ float Batch2DImpl::solve_packed(const cd* fields, cd* out) {
   downloaded_ = false;
   float ms = 0;
   check_cuda(cudaEventElapsedTime(&ms, ev_start_, ev_stop_), "elapsed");
+  check_status();
   return ms;
 }
 
@@ -1111,6 +1127,7 @@ void Batch2DImpl::download() {
   check_cuda(cudaMemcpyAsync(h_energy_.data(), d_energy_.ptr, d_energy_.bytes(), cudaMemcpyDeviceToHost, main_), "d2h");
   check_cuda(cudaMemcpyAsync(h_clock_.data(), d_clock_.ptr, d_clock_.bytes(), cudaMemcpyDeviceToHost, main_), "d2h");
   check_cuda(cudaStreamSynchronize(main_), "d2h");
+  check_status();
   downloaded_ = true;
 }
 

@@ -64,25 +64,93 @@ __device__ __forceinline__ int qreal(int j, int t, int c) {
   return C * (t + j * NT) + c;
 }
 
+// ---- exchanges through distributed shared memory -----------------------------------------------
+//
+// Each exchange is an all-to-all: every CTA sends values to every CTA of the cluster (itself
+// included) with st.async, an asynchronous remote store that also counts its bytes on the
+// receiver's mbarrier (complete_tx); the receiver has armed that mbarrier with the bytes it
+// expects and waits for the phase to complete. No cluster-wide barrier is needed, and a buffer
+// can be reused two exchanges later: a CTA sends exchange e + 2 only after receiving exchange
+// e + 1 from every peer, which each peer sent after reading its exchange-e data.
+struct Exchange {
+  cf* buf[2];         // receive buffers (alternating)
+  unsigned mbar[2];   // their mbarriers (shared-window addresses)
+  unsigned parity;    // bit b: parity of the phase awaited on buffer b
+  int cur;            // buffer of the next exchange
+  int* status;        // set to 1 when a wait gives up
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+// the same shared-memory offset in CTA `rank` of the cluster
+__device__ __forceinline__ unsigned mapa(unsigned addr, int rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_async(unsigned raddr, cf v, unsigned rmbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];"
+               :: "r"(raddr), "f"(v.re), "f"(v.im), "r"(rmbar) : "memory");
+}
+__device__ __forceinline__ void mbar_init(unsigned mbar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(mbar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned mbar, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}"
+               :: "r"(mbar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned mbar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+  return ok != 0;
+}
+
+// Opens the next exchange: thread 0 arms the receive mbarrier with the bytes to come.
+__device__ __forceinline__ void xopen(Exchange& ex, int t, unsigned bytes) {
+  if (t == 0) mbar_expect(ex.mbar[ex.cur], bytes);
+}
+
+// Waits for the current exchange's data, bounded: after 2 s the status word is set and the kernel
+// goes on with whatever arrived; once the word is set no later wait blocks, so a fault in the
+// protocol can neither hang the GPU nor stretch the run (its results are then reported invalid).
+__device__ __forceinline__ void xwait(Exchange& ex) {
+  const unsigned mb = ex.mbar[ex.cur], par = (ex.parity >> ex.cur) & 1u;
+  if (!mbar_try(mb, par) && *reinterpret_cast<volatile int*>(ex.status) == 0) {
+    const long long t0 = global_ns();
+    while (!mbar_try(mb, par)) {
+      if (global_ns() - t0 > 2000000000LL) {
+        atomicExch(ex.status, 1);
+        break;
+      }
+    }
+  }
+  ex.parity ^= 1u << ex.cur;
+  ex.cur ^= 1;
+}
+
 // Forward N-point transform: v holds the CTA's real-space values (owned pattern of the M-point
 // transform) and receives its spectral slots.
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
-                                        cf* const (&xb)[2], int& xphase, const Tw<float>* tw,
-                                        const Tw<float>* xf, const Tw<float>* xi, int t, int c,
-                                        cg::cluster_group& cl) {
+                                        Exchange& ex, const Tw<float>* tw, const Tw<float>* xf,
+                                        const Tw<float>* xi, int t, int c) {
   using S = Shape<N, C, NT>;
   rf::fft<-1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
-  cf* x = xb[xphase];
-  // push: Y_c[k1]·w_N^{c·k1} goes to the owner of k1's block (CTA j / EB, since
+  cf* x = ex.buf[ex.cur];
+  xopen(ex, t, S::M * sizeof(cf));
+  const unsigned base = smem_u32(x), mb = ex.mbar[ex.cur];
+  // Y_c[k1]·w_N^{c·k1} goes to the owner of k1's block (CTA j / EB, since
   // k1 = t + j·NT = (j / EB)·MB + (j mod EB)·NT + t), slot c·MB + (k1 mod MB) of its buffer
 #pragma unroll
   for (int j = 0; j < S::E; ++j) {
-    const int k1 = t + j * NT;
-    cf* dst = cl.map_shared_rank(x, j / S::EB);
-    dst[c * S::MB + (j % S::EB) * NT + t] = c == 0 ? v[j] : twmul<-1>(v[j], xf[k1]);
+    const int k1 = t + j * NT, dst = j / S::EB;
+    const unsigned off = static_cast<unsigned>(c * S::MB + (j % S::EB) * NT + t) * sizeof(cf);
+    st_async(mapa(base, dst) + off, c == 0 ? v[j] : twmul<-1>(v[j], xf[k1]), mapa(mb, dst));
   }
-  cl.sync();
+  xwait(ex);
 #pragma unroll
   for (int i = 0; i < S::EB; ++i) {
     const int k1l = i * NT + t;
@@ -93,17 +161,17 @@ __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) v[k2 * S::EB + i] = u[k2];
   }
-  xphase ^= 1;
 }
 
 // Inverse (unnormalised) N-point transform: spectral slots in, real-space owned values out.
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
-                                        cf* const (&xb)[2], int& xphase, const Tw<float>* tw,
-                                        const Tw<float>* xf, const Tw<float>* xi, int t, int c,
-                                        cg::cluster_group& cl) {
+                                        Exchange& ex, const Tw<float>* tw, const Tw<float>* xf,
+                                        const Tw<float>* xi, int t, int c) {
   using S = Shape<N, C, NT>;
-  cf* x = xb[xphase];
+  cf* x = ex.buf[ex.cur];
+  xopen(ex, t, S::M * sizeof(cf));
+  const unsigned base = smem_u32(x), mb = ex.mbar[ex.cur];
 #pragma unroll
   for (int i = 0; i < S::EB; ++i) {
     const int k1l = i * NT + t;
@@ -111,18 +179,16 @@ __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) u[k2] = v[k2 * S::EB + i];
     rf::dft<+1, C>(u);
-    // push Z_d[k1]·w_N^{−d·k1} (k1 = c·MB + k1l; the twiddle is entry d·M + k1l of
-    // xi = table + c·MB) to CTA d, slot k1 of its buffer
+    // Z_d[k1]·w_N^{−d·k1} (k1 = c·MB + k1l; the twiddle is entry d·M + k1l of
+    // xi = table + c·MB) goes to CTA d, slot k1 of its buffer
+    const unsigned off = static_cast<unsigned>(c * S::MB + k1l) * sizeof(cf);
 #pragma unroll
-    for (int d = 0; d < C; ++d) {
-      cf* dst = cl.map_shared_rank(x, d);
-      dst[c * S::MB + k1l] = d == 0 ? u[d] : twmul<+1>(u[d], xi[d * S::M + k1l]);
-    }
+    for (int d = 0; d < C; ++d)
+      st_async(mapa(base, d) + off, d == 0 ? u[d] : twmul<+1>(u[d], xi[d * S::M + k1l]), mapa(mb, d));
   }
-  cl.sync();
+  xwait(ex);
 #pragma unroll
   for (int j = 0; j < S::E; ++j) v[j] = x[t + j * NT];
-  xphase ^= 1;
   rf::fft<+1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
 }
 
@@ -175,12 +241,12 @@ __device__ __forceinline__ double flux(const cf (&v)[Shape<N, C, NT>::E], const 
 // values; mk: the mask of the CTA's points in shared memory, M hi then M lo values, or null).
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&out)[Shape<N, C, NT>::E],
-                                     cf* b0, cf* b1, int& phase, cf* const (&xb)[2], int& xphase,
+                                     cf* b0, cf* b1, int& phase, Exchange& ex,
                                      const R2Item& it, const R2Step& st, const R2Pass& p0,
                                      R2Next& nx, int next_p, bool next_backward, bool backward,
                                      bool reflect, cf* store, const cf* add, const float* mk,
                                      const Tw<float>* tw, const Tw<float>* xf, const Tw<float>* xi,
-                                     int t, int c, cg::cluster_group& cl) {
+                                     int t, int c) {
   using Sh = Shape<N, C, NT>;
   constexpr int E = Sh::E, M = Sh::M;
   const int off = backward ? st.bwd_off : st.fwd_off;
@@ -198,11 +264,11 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
       th[j] = m[k];
       tl[j] = m[N + k];
     }
-    forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+    forward<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
     if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = pmul(v[j], th[j], tl[j]);
-    inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+    inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
     if (mk)
 #pragma unroll
       for (int j = 0; j < E; ++j) {
@@ -210,7 +276,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
         v[j] = mask_mul(v[j], mk[m], mk[M + m]);
       }
   } else {
-    forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+    forward<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
     if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
 #pragma unroll
     for (int j = 0; j < E; ++j) S[rf::pad(t + j * NT)] = v[j];
@@ -222,7 +288,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
         const int k = kspec<N, C, NT>(j, t, c);
         v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
       }
-      inverse<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+      inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
       if (!ps.refl) {
 #pragma unroll
         for (int j = 0; j < E; ++j) {
@@ -277,7 +343,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   cf* b0 = reinterpret_cast<cf*>(smem_raw);
   cf* b1 = b0 + rf::padded(S::M);
   cf* Sl = b1 + rf::padded(S::M);
-  cf* const xb[2] = {Sl + rf::padded(S::M), Sl + rf::padded(S::M) + S::M};
+  __shared__ alignas(8) unsigned long long s_mbar[2];
   __shared__ int s_item;
   __shared__ double s_red[NT / 32];
   __shared__ double s_part;
@@ -290,7 +356,20 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   const Tw<float>* xf = xg + c * S::M;   // forward: this CTA's c, every k1
   const Tw<float>* xi = xg + c * S::MB;  // inverse: entry d·M + k1l for k1 = c·MB + k1l
   float* mask_s = reinterpret_cast<float*>(smem_raw + r2c::cluster_lines_bytes<N, C>());
-  int phase = 0, xphase = 0;
+  r2c::Exchange ex;
+  ex.buf[0] = Sl + rf::padded(S::M);
+  ex.buf[1] = ex.buf[0] + S::M;
+  ex.mbar[0] = r2c::smem_u32(&s_mbar[0]);
+  ex.mbar[1] = r2c::smem_u32(&s_mbar[1]);
+  ex.parity = 0;
+  ex.cur = 0;
+  ex.status = nullptr;
+  if (t == 0) {  // one arrival (thread 0's) per phase; visible to the peers after the first
+    r2c::mbar_init(ex.mbar[0], 1);  // cluster barrier below
+    r2c::mbar_init(ex.mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  int phase = 0;
   for (;;) {
     if (c == 0 && t == 0) s_item = atomicAdd(queue, 1);
     cl.sync();
@@ -300,6 +379,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
       return;
     }
     const R2Item it = items[idx];
+    ex.status = it.status;
     if (c == 0 && t == 0) it.clock[0] = global_ns();
     const float* mk = nullptr;
     if (it.mask) {  // first read in the first step's epilogue, after the transforms' barriers
@@ -314,7 +394,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
     const int iters = it.iterations > 0 ? it.iterations : 1;
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = it.input[r2c::qreal<N, C, NT>(j, t, c)];
-    r2c::forward<N, C, NT, RADS>(v, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+    r2c::forward<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
     {
       const double pin = r2c::flux<N, C, NT>(v, it.w_in, s_red, &s_part, t, c, cl);
       if (c == 0 && t == 0) it.energy[2 * iters] = pin;
@@ -343,9 +423,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, xb, xphase, it, st, p0, nx, next_p,
+        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, ex, it, st, p0, nx, next_p,
                                   next_backward, backward, reflect, store, add, mk, tw, xf, xi, t,
-                                  c, cl);
+                                  c);
       }
       cf* dst = backward ? it.reflected : it.transmitted;
 #pragma unroll
@@ -353,7 +433,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
       if (it.iterations == 0) break;
 #pragma unroll
       for (int j = 0; j < E; ++j) out[j] = v[j];
-      r2c::forward<N, C, NT, RADS>(out, b0, b1, phase, xb, xphase, tw, xf, xi, t, c, cl);
+      r2c::forward<N, C, NT, RADS>(out, b0, b1, phase, ex, tw, xf, xi, t, c);
       const double fl = r2c::flux<N, C, NT>(out, backward ? it.w_in : it.w_out, s_red, &s_part, t, c, cl);
       if (c == 0 && t == 0) it.energy[2 * iter + (backward ? 1 : 0)] = fl;
     }

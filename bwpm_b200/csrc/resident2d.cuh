@@ -50,6 +50,7 @@ struct R2Item {
   const double* w_in;     // (N) flux weight of the incident medium
   double* energy;         // (iterations, 2) transmitted/reflected flux, then the incident flux
   long long* clock;       // (2): start and end global timer, ns
+  int* status;            // the batch's status word: set to 1 when a bounded wait gave up
   int n, nz, iterations, plan;
 };
 
@@ -410,8 +411,10 @@ __device__ __forceinline__ int next_step(int s, int p, int nz, int sw, int sweep
   return -1;
 }
 
-template <int N, int NT, class RADS>
-__global__ void __launch_bounds__(NT, 1) k_resident2d_fixed(const R2Item* __restrict__ items,
+// MINB: CTAs per SM the register budget is sized for (1: up to 255 registers a thread; 2: two
+// items share an SM and hide each other's latencies, at the cost of registers).
+template <int N, int NT, class RADS, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_resident2d_fixed(const R2Item* __restrict__ items,
                                                          int nitems, int* queue,
                                                          const Tw<float>* __restrict__ tw) {
   constexpr int E = N / NT;

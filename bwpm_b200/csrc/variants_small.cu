@@ -11,6 +11,7 @@ template <int N, int NT, int... R>
 FixedVariant fixed() {
   return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>, fixed_smem_bytes<N>()};
 }
+
 }  // namespace
 
 void add_variants_small(std::vector<FixedVariant>& v) {
