@@ -45,9 +45,20 @@ template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_lines_bytes() {
   return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * (N / C)) * sizeof(cf) + 15) / 16 * 16;
 }
+// then the CTA's cross twiddles (forward w_N^{c·k1}, k1 < M; inverse w_N^{−d·k1} of its spectral
+// block, d < C) when they fit, loaded once per CTA
+template <int N, int C>
+__host__ __device__ constexpr std::size_t cluster_mask_end() {
+  return (cluster_lines_bytes<N, C>() + 2 * static_cast<std::size_t>(N / C) * sizeof(float) + 15) / 16 * 16;
+}
+template <int N, int C>
+__host__ __device__ constexpr bool cluster_xtw_in_smem() {
+  return cluster_mask_end<N, C>() + 2 * static_cast<std::size_t>(N / C) * sizeof(Tw<float>) <= 220 * 1024;
+}
 template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_smem_bytes() {
-  return cluster_lines_bytes<N, C>() + 2 * static_cast<std::size_t>(N / C) * sizeof(float);
+  return cluster_mask_end<N, C>() +
+         (cluster_xtw_in_smem<N, C>() ? 2 * static_cast<std::size_t>(N / C) * sizeof(Tw<float>) : 0);
 }
 
 // spectral index of slot s (= k2·EB + i) of thread t in CTA c
@@ -179,12 +190,14 @@ __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 #pragma unroll
     for (int k2 = 0; k2 < C; ++k2) u[k2] = v[k2 * S::EB + i];
     rf::dft<+1, C>(u);
-    // Z_d[k1]·w_N^{−d·k1} (k1 = c·MB + k1l; the twiddle is entry d·M + k1l of
-    // xi = table + c·MB) goes to CTA d, slot k1 of its buffer
+    // Z_d[k1]·w_N^{−d·k1} (k1 = c·MB + k1l; the twiddle is entry d·XS + k1l of xi: the CTA's
+    // staged block in shared memory, else the global table from entry c·MB) goes to CTA d,
+    // slot k1 of its buffer
+    constexpr int XS = cluster_xtw_in_smem<N, C>() ? S::MB : S::M;
     const unsigned off = static_cast<unsigned>(c * S::MB + k1l) * sizeof(cf);
 #pragma unroll
     for (int d = 0; d < C; ++d)
-      st_async(mapa(base, d) + off, d == 0 ? u[d] : twmul<+1>(u[d], xi[d * S::M + k1l]), mapa(mb, d));
+      st_async(mapa(base, d) + off, d == 0 ? u[d] : twmul<+1>(u[d], xi[d * XS + k1l]), mapa(mb, d));
   }
   xwait(ex);
 #pragma unroll
@@ -356,6 +369,16 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   const Tw<float>* xf = xg + c * S::M;   // forward: this CTA's c, every k1
   const Tw<float>* xi = xg + c * S::MB;  // inverse: entry d·M + k1l for k1 = c·MB + k1l
   float* mask_s = reinterpret_cast<float*>(smem_raw + r2c::cluster_lines_bytes<N, C>());
+  if constexpr (r2c::cluster_xtw_in_smem<N, C>()) {  // read first after the cluster barrier below
+    Tw<float>* xfs = reinterpret_cast<Tw<float>*>(smem_raw + r2c::cluster_mask_end<N, C>());
+    Tw<float>* xis = xfs + S::M;
+    for (int i = t; i < S::M; i += NT) {
+      xfs[i] = xf[i];
+      xis[i] = xi[(i / S::MB) * S::M + i % S::MB];
+    }
+    xf = xfs;
+    xi = xis;
+  }
   r2c::Exchange ex;
   ex.buf[0] = Sl + rf::padded(S::M);
   ex.buf[1] = ex.buf[0] + S::M;
