@@ -302,6 +302,12 @@ def run_ours(args) -> None:
     achieved = work["flops"] / kern_s / 1e12
     hbm_peak = _peak("hbm_gbs")
     served = run_served(device, args.served_fp64) if not args.no_served else None
+    configs = None
+    if not args.no_configs:
+        try:
+            configs = run_configs(device)
+        except Exception as e:  # noqa: BLE001 - a side measurement must not cost the headline
+            configs = {"error": f"{type(e).__name__}: {e}"}
     cb = cpu_baseline(params, budget_s=args.cpu_budget) if not args.no_cpu else None
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
@@ -335,6 +341,7 @@ def run_ours(args) -> None:
                      "hbm": {"achieved": work["bytes"] / kern_s / 1e9, "peak": hbm_peak,
                              "unit": "GB/s", "frac": work["bytes"] / kern_s / 1e9 / hbm_peak}},
         "served": served,
+        "configs": configs,
         "cpu_baseline": cb,
         "clocks": clocks,
         "setup_s": setup_s,
@@ -347,6 +354,11 @@ def run_ours(args) -> None:
 # ---- served request stream (continuous batching) ----------------------------------------------
 
 SERVED_COUNT, SERVED_MAX3D = 48, 256
+
+
+def _rel_floor(a, b, floor: float) -> float:
+    """‖a − b‖ / max(‖b‖, floor): relative error that stays meaningful for a vanishing field."""
+    return float(np.linalg.norm(a - b) / max(float(np.linalg.norm(b)), floor, 1e-300))
 
 
 def _rel(a, b) -> float:
@@ -409,6 +421,83 @@ def run_served(device: int, fp64_sample: int) -> dict:
     }
 
 
+# ---- the other configurations (parity and timing beside the headline; not part of its value) ----
+
+def run_configs(device: int) -> dict:
+    """Configurations 1-3 on this GPU: complex64 result of this implementation against the
+    per-solve FP64 drop-in path (time and relative L2 error), and for the 2D slab the reference's
+    CPU core on one thread. Born (configuration 2) runs on a reduced chain, stated in the entry."""
+    from bwpm_b200 import _core, workloads
+    from bwpm_b200.batch import Batch2D
+
+    def timed(fn):
+        t0 = time.perf_counter()
+        r = fn()
+        return r, time.perf_counter() - t0
+
+    out: dict = {}
+    # 1: 5 um slab, 1024 points, 250 slabs, 8 iterations, TE and TM
+    probs = [workloads.slab2d("te"), workloads.slab2d("tm")]
+    b = Batch2D(device)
+    ids = [b.add_problem(p) for p in probs]
+    b.prepare()
+    b.run()
+    batch_ms = b.run()
+    ref_core = None
+    so = sorted((ROOT / "oracle" / "_ref").glob("_core*.so"))
+    if so:
+        import importlib.util
+
+        spec = importlib.util.spec_from_file_location("_core", so[0])  # its init symbol
+        ref_core = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(ref_core)
+    t64, tcpu, errs = [], [], []
+    for p, i in zip(probs, ids):
+        r64, dt = timed(lambda p=p: _core.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))
+        t64.append(dt)
+        r32 = b.result(i)
+        errs += [_rel(r32["transmitted"], r64["transmitted"][:, 0]),
+                 _rel(r32["reflected"], r64["reflected"][:, 0])]
+        if ref_core is not None:
+            _, dt = timed(lambda p=p: ref_core.Solver(*p.core_args(), 1).run(p.field, p.iterations, []))
+            tcpu.append(dt)
+    out["slab2d"] = {"solves": 2, "c64_batched_ms_both": batch_ms,
+                     "fp64_ms_per_solve": 1e3 * float(np.mean(t64)),
+                     "cpu_reference_ms_per_solve": 1e3 * float(np.mean(tcpu)) if tcpu else None,
+                     "cpu_threads": 1, "l2_err_max": float(np.max(errs)),
+                     "workload": "1024 points, 250 slabs of lambda/10, 5 um slab n=1.5 in air, "
+                                 "8 iterations, TE and TM"}
+    # 3: microlens with a tilted silver back face, 512^2 points, 400 slabs, 6 iterations
+    p = workloads.microlens3d()
+    r32, t32 = timed(lambda: _core.CudaSolver(*p.core_args(), device, precision=32).run(p.field, p.iterations, []))
+    r64, t64s = timed(lambda: _core.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))
+    # the silver fills everything behind the back face: the transmitted field is ~1e-94 of the
+    # incident one in FP64, below the complex64 range, so errors are relative to the larger of
+    # the field's own norm and 1e-6 of the incident field's
+    floor = 1e-6 * float(np.linalg.norm(p.field))
+    out["microlens3d"] = {"c64_s": t32, "fp64_s": t64s,
+                          "l2_err": max(_rel_floor(r32["transmitted"], r64["transmitted"], floor),
+                                        _rel_floor(r32["reflected"], r64["reflected"], floor)),
+                          "l2_err_reflected": _rel(r32["reflected"], r64["reflected"]),
+                          "transmitted_norm_over_incident": float(np.linalg.norm(r64["transmitted"])) /
+                                                            float(np.linalg.norm(p.field)),
+                          "workload": "512^2 points, 400 slabs of lambda/8, lens n=1.52 + silver, "
+                                      "6 iterations; set-up (labels -> step records) included"}
+    del r32, r64, p
+    # 2 (reduced chain): Born fluctuation, 4096 points, 100 of the 2000 slabs, 1 of 6 iterations
+    p = workloads.born2d(nz=100, iterations=1)
+    r32, t32 = timed(lambda: _core.CudaSolver(*p.core_args(), device, fluctuation=p.fluctuation,
+                                              precision=32).run(p.field, p.iterations, []))
+    r64, t64s = timed(lambda: _core.CudaSolver(*p.core_args(), device,
+                                               fluctuation=p.fluctuation).run(p.field, p.iterations, []))
+    out["born2d_reduced"] = {"c64_s": t32, "fp64_s": t64s,
+                             "l2_err": max(_rel(r32["transmitted"], r64["transmitted"]),
+                                           _rel(r32["reflected"], r64["reflected"])),
+                             "workload": "4096 points, 100 of 2000 slabs, 1 of 6 iterations, "
+                                         "delta-n on every slab; set-up included"}
+    return out
+
+
 def prm_wl(prm: dict) -> float:
     return float(prm["wl"])
 
@@ -430,6 +519,7 @@ def main() -> None:
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="target CPU seconds per core")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip configurations 1-3")
     ap.add_argument("--served-fp64", type=int, default=6, help="FP64 sample of the served stream")
     ap.add_argument("--variants", type=str, default="",
                     help="profiling only: NY:VARIANT,... forces kernel variants (no autotuning)")
@@ -444,6 +534,7 @@ def main() -> None:
                        ny=vals[3] if len(vals) > 3 else None)
         args.no_cpu = True
         args.no_served = True
+        args.no_configs = True
         args.fp64_sample = 0
     if args.impl == "reference":
         run_reference(args)
