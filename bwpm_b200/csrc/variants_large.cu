@@ -12,11 +12,7 @@ template <int N, int NT, int... R>
 FixedVariant fixed() {
   return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>, fixed_smem_bytes<N>()};
 }
-// two CTAs per SM (registers capped for it)
-template <int N, int NT, int... R>
-FixedVariant fixed2() {
-  return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>, 2>, fixed_smem_bytes<N>()};
-}
+
 // one line over a cluster of C CTAs
 template <int N, int C, int NT, int... R>
 FixedVariant cluster() {
@@ -29,9 +25,7 @@ void add_variants_large(std::vector<FixedVariant>& v) {
   // per length, only variants that no other variant beats in both per-step latency and SM time
   // (measured on a B200: 1 item, tilted slab, 400 slabs); the first is the default
   v.push_back(fixed<2048, 256, 8, 8, 8, 4>());
-  v.push_back(fixed2<2048, 256, 8, 8, 8, 4>());
   v.push_back(fixed<3072, 256, 4, 4, 4, 4, 4, 3>());
-  v.push_back(fixed2<3072, 256, 4, 4, 4, 4, 4, 3>());
   v.push_back(fixed<4096, 256, 16, 16, 16>());
   v.push_back(cluster<4096, 2, 256, 8, 8, 8, 4>());
   v.push_back(cluster<4096, 4, 128, 8, 8, 8, 2>());

@@ -96,8 +96,9 @@ int bwpm_batch_add(bwpm_batch* b, size_t ny, double dy, double dz, double k0,
  * kernels (bwpm_variant_count(ny) > 0) have one or more variants (threads per CTA, FFT radices,
  * CTAs per line). on = 1: prepare picks them by timing the batch itself with every chain scaled
  * down to 1/4 of its slabs and one iteration (all lengths concurrently, as in a run),
- * coordinate descent from the first variants (a variant wins on a clearly faster batch, or on an
- * equal batch with clearly less SM time for its length). Default: the first variant. set_variant forces
+ * coordinate descent from the first variants and from the variants with the most CTAs per line,
+ * the better end kept (a variant wins on a clearly faster batch, or on an equal batch with
+ * clearly less SM time for its length). Default: the first variant. set_variant forces
  * variant `variant` (0-based) for length ny. */
 int bwpm_batch_set_autotune(bwpm_batch* b, int on);
 int bwpm_batch_set_variant(bwpm_batch* b, size_t ny, int variant);
