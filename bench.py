@@ -339,7 +339,8 @@ def run_ours(args) -> None:
                              "cores (FFT is not a dense contraction); peak = nominal FP32 "
                              "(no measured FP32 peak in MEASURED_PEAKS.json)",
                      "hbm": {"achieved": work["bytes"] / kern_s / 1e9, "peak": hbm_peak,
-                             "unit": "GB/s", "frac": work["bytes"] / kern_s / 1e9 / hbm_peak}},
+                             "unit": "GB/s", "frac": work["bytes"] / kern_s / 1e9 / hbm_peak,
+                             "peak_source": _peak_source()}},
         "served": served,
         "configs": configs,
         "cpu_baseline": cb,
@@ -500,6 +501,11 @@ def run_configs(device: int) -> dict:
 
 def prm_wl(prm: dict) -> float:
     return float(prm["wl"])
+
+
+def _peak_source() -> str:
+    """Where the HBM peak came from: the measured file of this pool, or the fallback figure."""
+    return "measured" if (ROOT / "MEASURED_PEAKS.json").exists() else "fallback (6.65 TB/s)"
 
 
 def _peak(key: str) -> float:
