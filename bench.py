@@ -40,9 +40,10 @@ COUNT, SEED = 256, 4
 REDUCED: dict = {}  # set by --reduced (profiling runs); empty for the benchmark itself
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs × FP32 lanes × FMA × max clock
 # DRAM bytes (read + write) of the class kernels of one batched run of this workload, summed
-# over the classes, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, default
-# kernel variants); the fields stay on chip, this is operator tables and pair ids L2 cannot hold
-TRAFFIC_PER_RUN_BYTES = 1.79e9
+# over the classes, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, kernel
+# variants of the autotuner); the fields stay on chip, this is operator tables and pair ids L2
+# cannot hold
+TRAFFIC_PER_RUN_BYTES = 1.72e9
 
 
 def _dist():
@@ -334,7 +335,7 @@ def run_ours(args) -> None:
                      "unit": "TFLOP/s", "frac": achieved / FP32_NOMINAL_TFLOPS,
                      "traffic": TRAFFIC_PER_RUN_BYTES if not REDUCED else None,
                      "traffic_note": "bytes per batched run (all class kernels), one ncu capture of "
-                                     "this workload with the default kernel variants",
+                                     "this workload with the autotuner's kernel variants",
                      "note": "shared-memory FFT: SIMT FP32 and shared-memory bound, no tensor "
                              "cores (FFT is not a dense contraction); peak = nominal FP32 "
                              "(no measured FP32 peak in MEASURED_PEAKS.json)",
