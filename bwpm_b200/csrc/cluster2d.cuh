@@ -9,16 +9,16 @@
 //   inverse:  Z_c[k1] = Σ_k2 X[k1 + M·k2]·w_C^{−c·k2}·w_N^{−c·k1};  exchange;
 //             x_c = IDFT_M(Z_c)
 // (a two-factor Cooley-Tukey split, N = M·C), each exchange one all-to-all through distributed
-// shared memory: every CTA stores its values straight into the owners' buffers (remote stores
-// need no round trip), one cluster barrier, then local reads. The local M-point transforms are
-// the register-resident transforms of rfft.cuh. Exchange buffers alternate, so one cluster
-// barrier per exchange suffices: a buffer is written again only after a later exchange's
-// barrier, which every CTA reaches after its reads of the earlier one.
+// shared memory: every CTA stores its values straight into the owners' buffers with st.async
+// (no round trip) and waits on its own mbarrier for the bytes it expects (see "exchanges"
+// below), then reads locally. The local M-point transforms are the register-resident transforms
+// of rfft.cuh.
 //
 // Everything else (passes, selection by pair id, mask, interface sources, FP64 flux) follows
 // k_resident2d_fixed; each CTA handles its own points. Cross twiddles w_N^{c·k1} (c < C,
 // k1 < M) are (hi, lo) pairs from FP64, stored after the M-point plan's twiddles (which hold
-// M − 1 entries for any radix order).
+// M − 1 entries for any radix order) and staged in the CTA's shared memory where they fit. The
+// item index and the flux partial sums go through cluster barriers (once per item and sweep).
 #pragma once
 
 #include <cooperative_groups.h>
