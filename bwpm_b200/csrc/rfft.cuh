@@ -135,20 +135,57 @@ __device__ __forceinline__ void stage(cf (&v)[N / NT], cf* buf, const Tw<float>*
   }
 }
 
+// A stage whose radix does not divide the values per thread E: the owned values go to in_buf,
+// each thread gathers whole butterflies i = t + j·NT < N/R (the last round partly idle), writes
+// their outputs to out_buf and reads back its owned values. Two barriers instead of one; the
+// caller leaves `phase` as it was (both buffers were used, the last reads were from out_buf).
+template <int DIR, int N, int NT, int R, int L, int OFF>
+__device__ __forceinline__ void stage_gather(cf (&v)[N / NT], cf* in_buf, cf* out_buf,
+                                             const Tw<float>* __restrict__ tw, int t) {
+  constexpr int E = N / NT, NB = N / R, KG = (NB + NT - 1) / NT;
+#pragma unroll
+  for (int m = 0; m < E; ++m) in_buf[pad(t + m * NT)] = v[m];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < KG; ++j) {
+    const int i = t + j * NT;
+    if (NB % NT == 0 || i < NB) {
+      const int k = i % L;
+      cf u[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) u[r] = in_buf[pad(i + r * NB)];
+      if constexpr (L > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) u[r] = twmul<DIR>(u[r], tw[OFF + (r - 1) * L + k]);
+      }
+      dft<DIR, R>(u);
+      const int base = (i - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) out_buf[pad(base + r * L)] = u[r];
+    }
+    asm volatile("" ::: "memory");
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < E; ++m) v[m] = out_buf[pad(t + m * NT)];
+}
+
 template <int DIR, int N, int NT, int L, int OFF, int R, int... Rest>
 __device__ __forceinline__ void stages(cf (&v)[N / NT], cf* b0, cf* b1, int& phase,
                                        const Tw<float>* __restrict__ tw, int t) {
   constexpr bool last = sizeof...(Rest) == 0;
-  stage<DIR, N, NT, R, L, OFF, last>(v, phase ? b1 : b0, tw, t);
-  if constexpr (!last) {
-    phase ^= 1;
-    stages<DIR, N, NT, L * R, OFF + L * (R - 1), Rest...>(v, b0, b1, phase, tw, t);
+  if constexpr ((N / NT) % R == 0) {
+    stage<DIR, N, NT, R, L, OFF, last>(v, phase ? b1 : b0, tw, t);
+    if constexpr (!last) phase ^= 1;
+  } else {
+    stage_gather<DIR, N, NT, R, L, OFF>(v, phase ? b1 : b0, phase ? b0 : b1, tw, t);
   }
+  if constexpr (!last) stages<DIR, N, NT, L * R, OFF + L * (R - 1), Rest...>(v, b0, b1, phase, tw, t);
 }
 
 // In-register transform of the owned values (DIR −1 forward, +1 inverse unnormalised).
-// `phase` selects the exchange buffer and must be uniform across the block; every exchange
-// flips it, so a later use of the buffers by the caller takes the buffer `phase` points to.
+// `phase` selects the exchange buffer and must be uniform across the block; the buffer it
+// points to after the transform is free for the caller (no thread still reads it).
 template <int DIR, int N, int NT, int... Rs>
 __device__ __forceinline__ void fft(cf (&v)[N / NT], cf* b0, cf* b1, int& phase,
                                    const Tw<float>* __restrict__ tw, int t, Radices<Rs...>) {

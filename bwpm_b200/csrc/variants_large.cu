@@ -32,7 +32,7 @@ void add_variants_large(std::vector<FixedVariant>& v) {
   v.push_back(cluster<4096, 8, 64, 8, 8, 8>());
   v.push_back(cluster<6144, 2, 256, 4, 4, 4, 4, 4, 3>());
   v.push_back(fixed<6144, 256, 8, 8, 8, 4, 3>());
-  v.push_back(cluster<6144, 4, 128, 4, 4, 4, 4, 2, 3>());
+  v.push_back(cluster<6144, 4, 192, 8, 8, 8, 3>());  // radix 3 as a gather stage
   v.push_back(cluster<8192, 4, 256, 8, 8, 8, 4>());
   v.push_back(fixed<8192, 512, 8, 8, 8, 8, 2>());
   v.push_back(cluster<8192, 8, 128, 8, 8, 8, 2>());

@@ -22,6 +22,7 @@ void add_variants_small(std::vector<FixedVariant>& v) {
   v.push_back(fixed<512, 64, 8, 8, 8>());
   v.push_back(fixed<768, 64, 4, 4, 4, 4, 3>());
   v.push_back(fixed<1024, 128, 8, 8, 8, 2>());
+  v.push_back(fixed<1536, 192, 8, 8, 8, 3>());  // radix 3 as a gather stage
   v.push_back(fixed<1536, 128, 4, 4, 4, 4, 2, 3>());
 }
 
