@@ -251,23 +251,27 @@ __device__ __forceinline__ double flux(const cf (&v)[Shape<N, C, NT>::E], const 
 }
 
 // One slab step of the CTA's share of an item (cf. r2f_step: prefetched records and operator
-// values; mk: the mask of the CTA's points in shared memory, M hi then M lo values, or null).
+// values, pair ids of the CTA's pixels loaded once per step, operator values of the next pass
+// prefetched into L1, first interface round loaded early; mk: the mask of the CTA's points in
+// shared memory, M hi then M lo values, or null).
 template <int N, int C, int NT, class RADS>
 __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&out)[Shape<N, C, NT>::E],
                                      cf* b0, cf* b1, int& phase, Exchange& ex,
                                      const R2Item& it, const R2Step& st, const R2Pass& p0,
-                                     R2Next& nx, int next_p, bool next_backward, bool backward,
-                                     bool reflect, cf* store, const cf* add, const float* mk,
-                                     const Tw<float>* tw, const Tw<float>* xf, const Tw<float>* xi,
-                                     int t, int c) {
+                                     const R2Pass& p1, R2Next& nx, int next_p, bool next_backward,
+                                     bool backward, bool reflect, cf* store, const cf* add,
+                                     const float* mk, const Tw<float>* tw, const Tw<float>* xf,
+                                     const Tw<float>* xi, int t, int c) {
   using Sh = Shape<N, C, NT>;
-  constexpr int E = Sh::E, M = Sh::M;
+  constexpr int E = Sh::E, M = Sh::M, EW = (E + 3) / 4;
   const int off = backward ? st.bwd_off : st.fwd_off;
-  const int ntp = backward ? st.bwd_t : st.fwd_t;
-  const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
+  const int npass = r2_passes(st, backward, reflect);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
   if (next_p >= 0) nx.st = it.steps[next_p];
+  const bool own_if = t < st.niface;
+  const int q0 = own_if ? iface[t] : 0;
+  const cf a0 = (add && own_if) ? add[t] : cf{0.f, 0.f};
   if (npass == 1) {
     const cf* m = it.tables + p0.tab;
     cf th[E], tl[E];  // in flight during the forward transform
@@ -278,7 +282,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
       tl[j] = m[N + k];
     }
     forward<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
-    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (next_p >= 0) r2_next_passes(nx, it, next_backward);
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = pmul(v[j], th[j], tl[j]);
     inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
@@ -289,37 +293,69 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
         v[j] = mask_mul(v[j], mk[m], mk[M + m]);
       }
   } else {
+    std::uint32_t pw[EW];
+    if (pid) {
+#pragma unroll
+      for (int w = 0; w < EW; ++w) pw[w] = 0;
+#pragma unroll
+      for (int j = 0; j < E; ++j)
+        pw[j >> 2] |= static_cast<std::uint32_t>(pid[qreal<N, C, NT>(j, t, c)]) << (8 * (j & 3));
+    }
+    {
+      const cf* m = it.tables + p0.tab;
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        const int k = kspec<N, C, NT>(j, t, c);
+        prefetch_l1(m + k);
+        prefetch_l1(m + N + k);
+      }
+    }
     forward<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
-    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (next_p >= 0) r2_next_passes(nx, it, next_backward);
+    const int pid0 = (pid && own_if) ? pid[q0] : 0;
 #pragma unroll
     for (int j = 0; j < E; ++j) S[rf::pad(t + j * NT)] = v[j];
+    R2Pass cur = p0, nxt = p1;
     for (int p = 0; p < npass; ++p) {
-      const R2Pass ps = p == 0 ? p0 : it.passes[off + p];
-      const cf* m = it.tables + ps.tab;
+      R2Pass nn = cur;
+      if (p + 2 < npass) nn = it.passes[off + p + 2];
+      if (p + 1 < npass) {
+        const cf* mn = it.tables + nxt.tab;
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+          const int k = kspec<N, C, NT>(j, t, c);
+          prefetch_l1(mn + k);
+          prefetch_l1(mn + N + k);
+        }
+      }
+      const cf* m = it.tables + cur.tab;
 #pragma unroll
       for (int j = 0; j < E; ++j) {
         const int k = kspec<N, C, NT>(j, t, c);
         v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
       }
       inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
-      if (!ps.refl) {
+      if (!cur.refl) {
 #pragma unroll
         for (int j = 0; j < E; ++j) {
-          const int q = qreal<N, C, NT>(j, t, c), ml = t + j * NT;
-          if (!pid || pid[q] == ps.pair) out[j] = mk ? mask_mul(v[j], mk[ml], mk[M + ml]) : v[j];
+          const int ml = t + j * NT;
+          if (!pid || unpack_pid<E>(pw, j) == cur.pair) out[j] = mk ? mask_mul(v[j], mk[ml], mk[M + ml]) : v[j];
         }
       } else {  // gather at this CTA's interface pixels through the free exchange buffer
         cf* buf = phase ? b1 : b0;
 #pragma unroll
         for (int j = 0; j < E; ++j) buf[rf::pad(t + j * NT)] = v[j];
         __syncthreads();
-        for (int k = t; k < st.niface; k += NT) {
+        if (own_if && q0 % C == c && (!pid || pid0 == cur.pair)) store[t] = buf[rf::pad(q0 / C)];
+        for (int k = t + NT; k < st.niface; k += NT) {
           const int q = iface[k];
           if (q % C != c) continue;
-          if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q / C)];
+          if (!pid || pid[q] == cur.pair) store[k] = buf[rf::pad(q / C)];
         }
         phase ^= 1;
       }
+      cur = nxt;
+      nxt = nn;
     }
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = out[j];
@@ -329,7 +365,11 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
 #pragma unroll
     for (int j = 0; j < E; ++j) buf[rf::pad(t + j * NT)] = v[j];
     __syncthreads();
-    for (int k = t; k < st.niface; k += NT) {
+    if (own_if && q0 % C == c) {
+      const int m = rf::pad(q0 / C);
+      buf[m] = buf[m] + a0;
+    }
+    for (int k = t + NT; k < st.niface; k += NT) {
       const int q = iface[k];
       if (q % C != c) continue;
       const int m = rf::pad(q / C);
@@ -425,7 +465,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
     const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
     R2Next nx;
     nx.st = it.steps[0];
-    nx.p0 = it.passes[nx.st.fwd_off];
+    r2_next_passes(nx, it, false);
     for (int sw = 0; sw < sweeps; ++sw) {
       const bool backward = sw & 1;
       const int iter = sw >> 1;
@@ -439,14 +479,14 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
       for (int s = 0; s < it.nz; ++s) {
         const int p = backward ? it.nz - 1 - s : s;
         const R2Step st = nx.st;
-        const R2Pass p0 = nx.p0;
+        const R2Pass p0 = nx.p0, p1 = nx.p1;
         bool next_backward;
         const int next_p = next_step(s, p, it.nz, sw, sweeps, backward, next_backward);
-        const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
+        const bool reflect = r2_reflects(st, backward, it.iterations);
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, ex, it, st, p0, nx, next_p,
+        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, ex, it, st, p0, p1, nx, next_p,
                                   next_backward, backward, reflect, store, add, mk, tw, xf, xi, t,
                                   c);
       }

@@ -295,7 +295,38 @@ __host__ __device__ constexpr std::size_t lines_bytes(int n, int lines) {
 struct R2Next {
   R2Step st;
   R2Pass p0;
+  R2Pass p1;  // second pass record, loaded only when the step has more than one pass
 };
+
+// Reflection passes run on a step with interface pixels in a backward sweep, and in a forward
+// sweep when the solve iterates (iterations > 0).
+__device__ __forceinline__ bool r2_reflects(const R2Step& st, bool backward, int iterations) {
+  return st.niface > 0 && (backward || iterations > 0);
+}
+
+// Passes of a step in one direction: its transmission passes, then its reflection passes.
+__device__ __forceinline__ int r2_passes(const R2Step& st, bool backward, bool reflect) {
+  return (backward ? st.bwd_t : st.fwd_t) + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
+}
+
+// The first pass record of the next step (nx.st has arrived), and its second when it has one.
+__device__ __forceinline__ void r2_next_passes(R2Next& nx, const R2Item& it, bool next_backward) {
+  const int off = next_backward ? nx.st.bwd_off : nx.st.fwd_off;
+  nx.p0 = it.passes[off];
+  if (r2_passes(nx.st, next_backward, r2_reflects(nx.st, next_backward, it.iterations)) > 1)
+    nx.p1 = it.passes[off + 1];
+}
+
+// Brings the L1 line holding p in from L2; holds no register while in flight.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// Pair id of owned value k from ids packed four to a 32-bit word.
+template <int E>
+__device__ __forceinline__ int unpack_pid(const std::uint32_t (&pw)[(E + 3) / 4], int k) {
+  return static_cast<int>((pw[k >> 2] >> (8 * (k & 3))) & 0xffu);
+}
 
 // The item's mask, (hi, lo) pairs, sits in shared memory beside the lines when it fits.
 template <int N>
@@ -307,24 +338,33 @@ __host__ __device__ constexpr std::size_t fixed_smem_bytes() {
   return lines_bytes(N, 3) + (fixed_mask_in_smem<N>() ? 2 * static_cast<std::size_t>(N) * sizeof(float) : 0);
 }
 
-// One slab step. st/p0: this step's record and first pass record (prefetched); nx receives the
-// records of step next_p (≥ 0) of direction next_backward. The spectrum of a multi-pass step is
-// kept in the shared line S at the owned positions (each thread reads back only what it wrote,
-// so S needs no barrier). mk: the item's mask (N hi values, then N lo values) or null.
+// One slab step. st/p0/p1: this step's record and first two pass records (prefetched; p1 is
+// valid when the step has more than one pass); nx receives the records of step next_p (≥ 0) of
+// direction next_backward. The spectrum of a multi-pass step is kept in the shared line S at the
+// owned positions (each thread reads back only what it wrote, so S needs no barrier). mk: the
+// item's mask (N hi values, then N lo values) or null.
+//
+// Latency of the multi-pass steps: the owned pixels' pair ids are loaded once per step (packed
+// in registers), the operator values of pass j + 1 are prefetched into L1 while pass j computes
+// (their record was loaded one pass earlier), and the first round of the interface loops (entry
+// t: pixel, its pair id, its added source) is loaded before the forward transform.
 template <int N, int NT, class RADS>
 __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / NT],
                                          cf* b0, cf* b1, int& phase, const R2Item& it,
-                                         const R2Step& st, const R2Pass& p0, R2Next& nx,
-                                         int next_p, bool next_backward, bool backward,
+                                         const R2Step& st, const R2Pass& p0, const R2Pass& p1,
+                                         R2Next& nx, int next_p, bool next_backward, bool backward,
                                          bool reflect, cf* store, const cf* add, const float* mk,
                                          const Tw<float>* __restrict__ tw, int t) {
-  constexpr int E = N / NT;
+  constexpr int E = N / NT, EW = (E + 3) / 4;
   const int off = backward ? st.bwd_off : st.fwd_off;
-  const int ntp = backward ? st.bwd_t : st.fwd_t;
-  const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
+  const int npass = r2_passes(st, backward, reflect);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
   if (next_p >= 0) nx.st = it.steps[next_p];
+  // interface entry t, the first round of the gather and add loops
+  const bool own_if = t < st.niface;
+  const int q0 = own_if ? iface[t] : 0;
+  const cf a0 = (add && own_if) ? add[t] : cf{0.f, 0.f};
   if (npass == 1) {  // one transmission pass over every pixel
     // operator values first: their loads are in flight during the forward transform
     const cf* m = it.tables + p0.tab;
@@ -335,7 +375,7 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
       tl[k] = m[N + t + k * NT];
     }
     rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
-    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (next_p >= 0) r2_next_passes(nx, it, next_backward);
 #pragma unroll
     for (int k = 0; k < E; ++k) v[k] = pmul(v[k], th[k], tl[k]);
     rf::fft<+1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
@@ -346,13 +386,39 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
         v[k] = mask_mul(v[k], mk[q], mk[N + q]);
       }
   } else {
+    std::uint32_t pw[EW];
+    if (pid) {
+#pragma unroll
+      for (int w = 0; w < EW; ++w) pw[w] = 0;
+#pragma unroll
+      for (int k = 0; k < E; ++k) pw[k >> 2] |= static_cast<std::uint32_t>(pid[t + k * NT]) << (8 * (k & 3));
+    }
+    {
+      const cf* m = it.tables + p0.tab;
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        prefetch_l1(m + t + k * NT);
+        prefetch_l1(m + N + t + k * NT);
+      }
+    }
     rf::fft<-1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
-    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (next_p >= 0) r2_next_passes(nx, it, next_backward);
+    const int pid0 = (pid && own_if) ? pid[q0] : 0;
 #pragma unroll
     for (int k = 0; k < E; ++k) S[rf::pad(t + k * NT)] = v[k];
+    R2Pass cur = p0, nxt = p1;
     for (int j = 0; j < npass; ++j) {
-      const R2Pass ps = j == 0 ? p0 : it.passes[off + j];
-      const cf* m = it.tables + ps.tab;
+      R2Pass nn = cur;
+      if (j + 2 < npass) nn = it.passes[off + j + 2];
+      if (j + 1 < npass) {
+        const cf* mn = it.tables + nxt.tab;
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+          prefetch_l1(mn + t + k * NT);
+          prefetch_l1(mn + N + t + k * NT);
+        }
+      }
+      const cf* m = it.tables + cur.tab;
 #pragma unroll
       for (int k = 0; k < E; ++k) {
         const int q = t + k * NT;
@@ -360,11 +426,11 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
         if ((k & 3) == 3) asm volatile("" ::: "memory");
       }
       rf::fft<+1, N, NT>(v, b0, b1, phase, tw, t, RADS{});
-      if (!ps.refl) {
+      if (!cur.refl) {
 #pragma unroll
         for (int k = 0; k < E; ++k) {
           const int q = t + k * NT;
-          if (!pid || pid[q] == ps.pair) out[k] = mk ? mask_mul(v[k], mk[q], mk[N + q]) : v[k];
+          if (!pid || unpack_pid<E>(pw, k) == cur.pair) out[k] = mk ? mask_mul(v[k], mk[q], mk[N + q]) : v[k];
           if ((k & 3) == 3) asm volatile("" ::: "memory");
         }
       } else {  // gather at the interface pixels through the free exchange buffer
@@ -372,12 +438,15 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
 #pragma unroll
         for (int k = 0; k < E; ++k) buf[rf::pad(t + k * NT)] = v[k];
         __syncthreads();
-        for (int k = t; k < st.niface; k += NT) {
+        if (own_if && (!pid || pid0 == cur.pair)) store[t] = buf[rf::pad(q0)];
+        for (int k = t + NT; k < st.niface; k += NT) {
           const int q = iface[k];
-          if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q)];
+          if (!pid || pid[q] == cur.pair) store[k] = buf[rf::pad(q)];
         }
         phase ^= 1;
       }
+      cur = nxt;
+      nxt = nn;
     }
 #pragma unroll
     for (int k = 0; k < E; ++k) v[k] = out[k];
@@ -387,7 +456,11 @@ __device__ __forceinline__ void r2f_step(cf (&v)[N / NT], cf* S, cf (&out)[N / N
 #pragma unroll
     for (int k = 0; k < E; ++k) buf[rf::pad(t + k * NT)] = v[k];
     __syncthreads();
-    for (int k = t; k < st.niface; k += NT) {
+    if (own_if) {
+      const int q = rf::pad(q0);
+      buf[q] = buf[q] + a0;
+    }
+    for (int k = t + NT; k < st.niface; k += NT) {
       const int q = rf::pad(iface[k]);
       buf[q] = buf[q] + add[k];
     }
@@ -453,7 +526,7 @@ __global__ void __launch_bounds__(NT, MINB) k_resident2d_fixed(const R2Item* __r
     const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
     R2Next nx;
     nx.st = it.steps[0];
-    nx.p0 = it.passes[nx.st.fwd_off];
+    r2_next_passes(nx, it, false);
     for (int sw = 0; sw < sweeps; ++sw) {
       const bool backward = sw & 1;
       const int iter = sw >> 1;
@@ -466,15 +539,15 @@ __global__ void __launch_bounds__(NT, MINB) k_resident2d_fixed(const R2Item* __r
       for (int s = 0; s < it.nz; ++s) {
         const int p = backward ? it.nz - 1 - s : s;  // step p: planes p and p + 1
         const R2Step st = nx.st;
-        const R2Pass p0 = nx.p0;
+        const R2Pass p0 = nx.p0, p1 = nx.p1;
         bool next_backward;
         const int next_p = next_step(s, p, it.nz, sw, sweeps, backward, next_backward);
-        const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
+        const bool reflect = r2_reflects(st, backward, it.iterations);
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        r2f_step<N, NT, RADS>(v, S, out, b0, b1, phase, it, st, p0, nx, next_p, next_backward,
-                              backward, reflect, store, add, mk, tw, t);
+        r2f_step<N, NT, RADS>(v, S, out, b0, b1, phase, it, st, p0, p1, nx, next_p,
+                              next_backward, backward, reflect, store, add, mk, tw, t);
       }
       r2f_store<N, NT>(backward ? it.reflected : it.transmitted, v, t);
       if (it.iterations == 0) break;
