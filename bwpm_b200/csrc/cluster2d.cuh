@@ -39,26 +39,46 @@ struct Shape {
   static_assert(N % C == 0 && M % NT == 0 && E % C == 0, "cluster shape");
 };
 
-// Shared memory of a cluster kernel: three padded lines and two exchange buffers of M points,
-// then the mask of the CTA's points (M hi values, M lo values).
+// Shared memory of a cluster kernel: three padded lines and two exchange buffers of G·M points
+// (G: passes per exchange), then the mask of the CTA's points (M hi values, M lo values), then
+// the CTA's cross twiddles (forward w_N^{c·k1}, k1 < M; inverse w_N^{−d·k1} of its spectral block,
+// d < C) when they fit, loaded once per CTA.
+template <int N, int C>
+__host__ __device__ constexpr std::size_t cluster_base_bytes(int g) {
+  return ((static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * g * (N / C)) * sizeof(cf) + 15) / 16 * 16 +
+          2 * static_cast<std::size_t>(N / C) * sizeof(float) + 15) / 16 * 16;
+}
+template <int N, int C>
+__host__ __device__ constexpr std::size_t cluster_xtw_bytes() {
+  return 2 * static_cast<std::size_t>(N / C) * sizeof(Tw<float>);
+}
+constexpr std::size_t kClusterSmemCap = 220 * 1024;
+// Passes per inverse exchange: the largest G ≤ 4 that fits with the cross twiddles in shared
+// memory, else the largest that fits without them.
+template <int N, int C>
+__host__ __device__ constexpr int cluster_group() {
+  for (int g = 4; g >= 1; --g)
+    if (cluster_base_bytes<N, C>(g) + cluster_xtw_bytes<N, C>() <= kClusterSmemCap) return g;
+  for (int g = 4; g >= 1; --g)
+    if (cluster_base_bytes<N, C>(g) <= kClusterSmemCap) return g;
+  return 1;
+}
 template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_lines_bytes() {
-  return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * (N / C)) * sizeof(cf) + 15) / 16 * 16;
+  return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * cluster_group<N, C>() * (N / C)) * sizeof(cf) +
+          15) / 16 * 16;
 }
-// then the CTA's cross twiddles (forward w_N^{c·k1}, k1 < M; inverse w_N^{−d·k1} of its spectral
-// block, d < C) when they fit, loaded once per CTA
 template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_mask_end() {
-  return (cluster_lines_bytes<N, C>() + 2 * static_cast<std::size_t>(N / C) * sizeof(float) + 15) / 16 * 16;
+  return cluster_base_bytes<N, C>(cluster_group<N, C>());
 }
 template <int N, int C>
 __host__ __device__ constexpr bool cluster_xtw_in_smem() {
-  return cluster_mask_end<N, C>() + 2 * static_cast<std::size_t>(N / C) * sizeof(Tw<float>) <= 220 * 1024;
+  return cluster_mask_end<N, C>() + cluster_xtw_bytes<N, C>() <= kClusterSmemCap;
 }
 template <int N, int C>
 __host__ __device__ constexpr std::size_t cluster_smem_bytes() {
-  return cluster_mask_end<N, C>() +
-         (cluster_xtw_in_smem<N, C>() ? 2 * static_cast<std::size_t>(N / C) * sizeof(Tw<float>) : 0);
+  return cluster_mask_end<N, C>() + (cluster_xtw_in_smem<N, C>() ? cluster_xtw_bytes<N, C>() : 0);
 }
 
 // spectral index of slot s (= k2·EB + i) of thread t in CTA c
@@ -82,7 +102,10 @@ __device__ __forceinline__ int qreal(int j, int t, int c) {
 // receiver's mbarrier (complete_tx); the receiver has armed that mbarrier with the bytes it
 // expects and waits for the phase to complete. No cluster-wide barrier is needed, and a buffer
 // can be reused two exchanges later: a CTA sends exchange e + 2 only after receiving exchange
-// e + 1 from every peer, which each peer sent after reading its exchange-e data.
+// e + 1 from every peer, which each peer sent after reading its exchange-e data. An exchange
+// costs a DSMEM round of latency (≈ 0.5 µs), not bandwidth, so the inverse transforms of a
+// multi-pass step share one: up to G passes go out into slots q·M of the receive buffer and the
+// CTA waits once for g·M values.
 struct Exchange {
   cf* buf[2];         // receive buffers (alternating)
   unsigned mbar[2];   // their mbarriers (shared-window addresses)
@@ -125,16 +148,24 @@ __device__ __forceinline__ void xopen(Exchange& ex, int t, unsigned bytes) {
 }
 
 // Waits for the current exchange's data, bounded: after 2 s the status word is set and the kernel
-// goes on with whatever arrived; once the word is set no later wait blocks, so a fault in the
-// protocol can neither hang the GPU nor stretch the run (its results are then reported invalid).
+// goes on with whatever arrived. The status word is read only on the slow path (every 20 µs of
+// waiting; a global load on the fast path would put an L2 round trip into every exchange): once
+// it is set, a later wait gives up within 20 µs, so a fault in the protocol can neither hang the
+// GPU nor stretch the run far (its results are then reported invalid).
 __device__ __forceinline__ void xwait(Exchange& ex) {
   const unsigned mb = ex.mbar[ex.cur], par = (ex.parity >> ex.cur) & 1u;
-  if (!mbar_try(mb, par) && *reinterpret_cast<volatile int*>(ex.status) == 0) {
+  if (!mbar_try(mb, par)) {
     const long long t0 = global_ns();
+    long long check = 20000;
     while (!mbar_try(mb, par)) {
-      if (global_ns() - t0 > 2000000000LL) {
-        atomicExch(ex.status, 1);
-        break;
+      const long long dt = global_ns() - t0;
+      if (dt > check) {
+        if (*reinterpret_cast<volatile int*>(ex.status) != 0) break;
+        if (dt > 2000000000LL) {
+          atomicExch(ex.status, 1);
+          break;
+        }
+        check = dt + 20000;
       }
     }
   }
@@ -174,15 +205,14 @@ __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
   }
 }
 
-// Inverse (unnormalised) N-point transform: spectral slots in, real-space owned values out.
-template <int N, int C, int NT, class RADS>
-__device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
-                                        Exchange& ex, const Tw<float>* tw, const Tw<float>* xf,
-                                        const Tw<float>* xi, int t, int c) {
+// First half of an inverse (unnormalised) N-point transform: the C-point inverse DFTs of the
+// spectral slots, the cross twiddles, and the values sent to group slot q (offset q·M) of every
+// CTA's current receive buffer. The caller opens the exchange for all its slots and waits once.
+template <int N, int C, int NT>
+__device__ __forceinline__ void inverse_send(const cf (&v)[Shape<N, C, NT>::E], const Exchange& ex,
+                                             int q, const Tw<float>* xi, int t, int c) {
   using S = Shape<N, C, NT>;
-  cf* x = ex.buf[ex.cur];
-  xopen(ex, t, S::M * sizeof(cf));
-  const unsigned base = smem_u32(x), mb = ex.mbar[ex.cur];
+  const unsigned base = smem_u32(ex.buf[ex.cur] + q * S::M), mb = ex.mbar[ex.cur];
 #pragma unroll
   for (int i = 0; i < S::EB; ++i) {
     const int k1l = i * NT + t;
@@ -199,10 +229,29 @@ __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
     for (int d = 0; d < C; ++d)
       st_async(mapa(base, d) + off, d == 0 ? u[d] : twmul<+1>(u[d], xi[d * XS + k1l]), mapa(mb, d));
   }
-  xwait(ex);
+}
+
+// Second half: the received slot x (M points) to the real-space owned values.
+template <int N, int C, int NT, class RADS>
+__device__ __forceinline__ void inverse_finish(cf (&v)[Shape<N, C, NT>::E], const cf* x, cf* b0,
+                                               cf* b1, int& phase, const Tw<float>* tw, int t) {
+  using S = Shape<N, C, NT>;
 #pragma unroll
   for (int j = 0; j < S::E; ++j) v[j] = x[t + j * NT];
   rf::fft<+1, S::M, NT>(v, b0, b1, phase, tw, t, RADS{});
+}
+
+// Inverse (unnormalised) N-point transform: spectral slots in, real-space owned values out.
+template <int N, int C, int NT, class RADS>
+__device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
+                                        Exchange& ex, const Tw<float>* tw, const Tw<float>* xi,
+                                        int t, int c) {
+  using S = Shape<N, C, NT>;
+  const cf* x = ex.buf[ex.cur];
+  xopen(ex, t, S::M * sizeof(cf));
+  inverse_send<N, C, NT>(v, ex, 0, xi, t, c);
+  xwait(ex);
+  inverse_finish<N, C, NT, RADS>(v, x, b0, b1, phase, tw, t);
 }
 
 // Σ w[k]·|v|² over the CTA's spectral slots, compensated FP64; the cluster total is returned on
@@ -250,6 +299,16 @@ __device__ __forceinline__ double flux(const cf (&v)[Shape<N, C, NT>::E], const 
   return total;
 }
 
+// Record q of a group held in registers (selects with constant indices, no local memory).
+template <int G>
+__device__ __forceinline__ R2Pass pick(const R2Pass (&r)[G], int q) {
+  R2Pass x = r[0];
+#pragma unroll
+  for (int i = 1; i < G; ++i)
+    if (q == i) x = r[i];
+  return x;
+}
+
 // One slab step of the CTA's share of an item (cf. r2f_step: prefetched records and operator
 // values, pair ids of the CTA's pixels loaded once per step, operator values of the next pass
 // prefetched into L1, first interface round loaded early; mk: the mask of the CTA's points in
@@ -285,7 +344,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
     if (next_p >= 0) r2_next_passes(nx, it, next_backward);
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = pmul(v[j], th[j], tl[j]);
-    inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
+    inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xi, t, c);
     if (mk)
 #pragma unroll
       for (int j = 0; j < E; ++j) {
@@ -293,6 +352,9 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
         v[j] = mask_mul(v[j], mk[m], mk[M + m]);
       }
   } else {
+    // passes in groups of G: spectral multiply and send every pass of the group into its slot
+    // of the receive buffer, wait once, then the local inverse transforms and epilogues
+    constexpr int G = cluster_group<N, C>();
     std::uint32_t pw[EW];
     if (pid) {
 #pragma unroll
@@ -301,8 +363,17 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
       for (int j = 0; j < E; ++j)
         pw[j >> 2] |= static_cast<std::uint32_t>(pid[qreal<N, C, NT>(j, t, c)]) << (8 * (j & 3));
     }
-    {
-      const cf* m = it.tables + p0.tab;
+    // the first group's records: p0 and p1 came with the step record, the others load now
+    R2Pass rec[G];
+#pragma unroll
+    for (int q = 0; q < G; ++q) rec[q] = p0;
+    if constexpr (G > 1) rec[1] = p1;
+#pragma unroll
+    for (int q = 2; q < G; ++q)
+      if (q < npass) rec[q] = it.passes[off + q];
+#pragma unroll
+    for (int q = 0; q < (G < 2 ? G : 2); ++q) {
+      const cf* m = it.tables + rec[q].tab;
 #pragma unroll
       for (int j = 0; j < E; ++j) {
         const int k = kspec<N, C, NT>(j, t, c);
@@ -314,48 +385,62 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
     if (next_p >= 0) r2_next_passes(nx, it, next_backward);
     const int pid0 = (pid && own_if) ? pid[q0] : 0;
 #pragma unroll
-    for (int j = 0; j < E; ++j) S[rf::pad(t + j * NT)] = v[j];
-    R2Pass cur = p0, nxt = p1;
-    for (int p = 0; p < npass; ++p) {
-      R2Pass nn = cur;
-      if (p + 2 < npass) nn = it.passes[off + p + 2];
-      if (p + 1 < npass) {
-        const cf* mn = it.tables + nxt.tab;
+    for (int q = 2; q < G; ++q)
+      if (q < npass) {
+        const cf* m = it.tables + rec[q].tab;
 #pragma unroll
         for (int j = 0; j < E; ++j) {
           const int k = kspec<N, C, NT>(j, t, c);
-          prefetch_l1(mn + k);
-          prefetch_l1(mn + N + k);
+          prefetch_l1(m + k);
+          prefetch_l1(m + N + k);
         }
       }
-      const cf* m = it.tables + cur.tab;
 #pragma unroll
-      for (int j = 0; j < E; ++j) {
-        const int k = kspec<N, C, NT>(j, t, c);
-        v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
+    for (int j = 0; j < E; ++j) S[rf::pad(t + j * NT)] = v[j];
+    for (int p = 0; p < npass; p += G) {
+      const int g = npass - p < G ? npass - p : G;
+      if (p > 0) {  // later groups (steps with more than G passes)
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+          if (q < g) rec[q] = it.passes[off + p + q];
       }
-      inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xf, xi, t, c);
-      if (!cur.refl) {
+      const cf* x = ex.buf[ex.cur];
+      xopen(ex, t, static_cast<unsigned>(g * M) * sizeof(cf));
+#pragma unroll 1
+      for (int q = 0; q < g; ++q) {
+        const cf* m = it.tables + pick(rec, q).tab;
 #pragma unroll
         for (int j = 0; j < E; ++j) {
-          const int ml = t + j * NT;
-          if (!pid || unpack_pid<E>(pw, j) == cur.pair) out[j] = mk ? mask_mul(v[j], mk[ml], mk[M + ml]) : v[j];
+          const int k = kspec<N, C, NT>(j, t, c);
+          v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
         }
-      } else {  // gather at this CTA's interface pixels through the free exchange buffer
-        cf* buf = phase ? b1 : b0;
-#pragma unroll
-        for (int j = 0; j < E; ++j) buf[rf::pad(t + j * NT)] = v[j];
-        __syncthreads();
-        if (own_if && q0 % C == c && (!pid || pid0 == cur.pair)) store[t] = buf[rf::pad(q0 / C)];
-        for (int k = t + NT; k < st.niface; k += NT) {
-          const int q = iface[k];
-          if (q % C != c) continue;
-          if (!pid || pid[q] == cur.pair) store[k] = buf[rf::pad(q / C)];
-        }
-        phase ^= 1;
+        inverse_send<N, C, NT>(v, ex, q, xi, t, c);
       }
-      cur = nxt;
-      nxt = nn;
+      xwait(ex);
+#pragma unroll 1
+      for (int q = 0; q < g; ++q) {
+        const R2Pass cur = pick(rec, q);
+        inverse_finish<N, C, NT, RADS>(v, x + q * M, b0, b1, phase, tw, t);
+        if (!cur.refl) {
+#pragma unroll
+          for (int j = 0; j < E; ++j) {
+            const int ml = t + j * NT;
+            if (!pid || unpack_pid<E>(pw, j) == cur.pair) out[j] = mk ? mask_mul(v[j], mk[ml], mk[M + ml]) : v[j];
+          }
+        } else {  // gather at this CTA's interface pixels through the free transform buffer
+          cf* buf = phase ? b1 : b0;
+#pragma unroll
+          for (int j = 0; j < E; ++j) buf[rf::pad(t + j * NT)] = v[j];
+          __syncthreads();
+          if (own_if && q0 % C == c && (!pid || pid0 == cur.pair)) store[t] = buf[rf::pad(q0 / C)];
+          for (int k = t + NT; k < st.niface; k += NT) {
+            const int qq = iface[k];
+            if (qq % C != c) continue;
+            if (!pid || pid[qq] == cur.pair) store[k] = buf[rf::pad(qq / C)];
+          }
+          phase ^= 1;
+        }
+      }
     }
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = out[j];
@@ -421,7 +506,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   }
   r2c::Exchange ex;
   ex.buf[0] = Sl + rf::padded(S::M);
-  ex.buf[1] = ex.buf[0] + S::M;
+  ex.buf[1] = ex.buf[0] + r2c::cluster_group<N, C>() * S::M;
   ex.mbar[0] = r2c::smem_u32(&s_mbar[0]);
   ex.mbar[1] = r2c::smem_u32(&s_mbar[1]);
   ex.parity = 0;
