@@ -63,22 +63,22 @@ __host__ __device__ constexpr int cluster_group() {
     if (cluster_base_bytes<N, C>(g) <= kClusterSmemCap) return g;
   return 1;
 }
-template <int N, int C>
+// (a variant may take a smaller G, so that two CTAs fit on one SM)
+template <int N, int C, int G>
 __host__ __device__ constexpr std::size_t cluster_lines_bytes() {
-  return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * cluster_group<N, C>() * (N / C)) * sizeof(cf) +
-          15) / 16 * 16;
+  return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * G * (N / C)) * sizeof(cf) + 15) / 16 * 16;
 }
-template <int N, int C>
+template <int N, int C, int G>
 __host__ __device__ constexpr std::size_t cluster_mask_end() {
-  return cluster_base_bytes<N, C>(cluster_group<N, C>());
+  return cluster_base_bytes<N, C>(G);
 }
-template <int N, int C>
+template <int N, int C, int G>
 __host__ __device__ constexpr bool cluster_xtw_in_smem() {
-  return cluster_mask_end<N, C>() + cluster_xtw_bytes<N, C>() <= kClusterSmemCap;
+  return cluster_mask_end<N, C, G>() + cluster_xtw_bytes<N, C>() <= kClusterSmemCap;
 }
-template <int N, int C>
+template <int N, int C, int G>
 __host__ __device__ constexpr std::size_t cluster_smem_bytes() {
-  return cluster_mask_end<N, C>() + (cluster_xtw_in_smem<N, C>() ? cluster_xtw_bytes<N, C>() : 0);
+  return cluster_mask_end<N, C, G>() + (cluster_xtw_in_smem<N, C, G>() ? cluster_xtw_bytes<N, C>() : 0);
 }
 
 // spectral index of slot s (= k2·EB + i) of thread t in CTA c
@@ -208,7 +208,7 @@ __device__ __forceinline__ void forward(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf*
 // First half of an inverse (unnormalised) N-point transform: the C-point inverse DFTs of the
 // spectral slots, the cross twiddles, and the values sent to group slot q (offset q·M) of every
 // CTA's current receive buffer. The caller opens the exchange for all its slots and waits once.
-template <int N, int C, int NT>
+template <int N, int C, int NT, int G>
 __device__ __forceinline__ void inverse_send(const cf (&v)[Shape<N, C, NT>::E], const Exchange& ex,
                                              int q, const Tw<float>* xi, int t, int c) {
   using S = Shape<N, C, NT>;
@@ -223,7 +223,7 @@ __device__ __forceinline__ void inverse_send(const cf (&v)[Shape<N, C, NT>::E], 
     // Z_d[k1]·w_N^{−d·k1} (k1 = c·MB + k1l; the twiddle is entry d·XS + k1l of xi: the CTA's
     // staged block in shared memory, else the global table from entry c·MB) goes to CTA d,
     // slot k1 of its buffer
-    constexpr int XS = cluster_xtw_in_smem<N, C>() ? S::MB : S::M;
+    constexpr int XS = cluster_xtw_in_smem<N, C, G>() ? S::MB : S::M;
     const unsigned off = static_cast<unsigned>(c * S::MB + k1l) * sizeof(cf);
 #pragma unroll
     for (int d = 0; d < C; ++d)
@@ -242,14 +242,14 @@ __device__ __forceinline__ void inverse_finish(cf (&v)[Shape<N, C, NT>::E], cons
 }
 
 // Inverse (unnormalised) N-point transform: spectral slots in, real-space owned values out.
-template <int N, int C, int NT, class RADS>
+template <int N, int C, int NT, class RADS, int G>
 __device__ __forceinline__ void inverse(cf (&v)[Shape<N, C, NT>::E], cf* b0, cf* b1, int& phase,
                                         Exchange& ex, const Tw<float>* tw, const Tw<float>* xi,
                                         int t, int c) {
   using S = Shape<N, C, NT>;
   const cf* x = ex.buf[ex.cur];
   xopen(ex, t, S::M * sizeof(cf));
-  inverse_send<N, C, NT>(v, ex, 0, xi, t, c);
+  inverse_send<N, C, NT, G>(v, ex, 0, xi, t, c);
   xwait(ex);
   inverse_finish<N, C, NT, RADS>(v, x, b0, b1, phase, tw, t);
 }
@@ -313,7 +313,7 @@ __device__ __forceinline__ R2Pass pick(const R2Pass (&r)[G], int q) {
 // values, pair ids of the CTA's pixels loaded once per step, operator values of the next pass
 // prefetched into L1, first interface round loaded early; mk: the mask of the CTA's points in
 // shared memory, M hi then M lo values, or null).
-template <int N, int C, int NT, class RADS>
+template <int N, int C, int NT, class RADS, int G>
 __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&out)[Shape<N, C, NT>::E],
                                      cf* b0, cf* b1, int& phase, Exchange& ex,
                                      const R2Item& it, const R2Step& st, const R2Pass& p0,
@@ -344,7 +344,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
     if (next_p >= 0) r2_next_passes(nx, it, next_backward);
 #pragma unroll
     for (int j = 0; j < E; ++j) v[j] = pmul(v[j], th[j], tl[j]);
-    inverse<N, C, NT, RADS>(v, b0, b1, phase, ex, tw, xi, t, c);
+    inverse<N, C, NT, RADS, G>(v, b0, b1, phase, ex, tw, xi, t, c);
     if (mk)
 #pragma unroll
       for (int j = 0; j < E; ++j) {
@@ -354,7 +354,6 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
   } else {
     // passes in groups of G: spectral multiply and send every pass of the group into its slot
     // of the receive buffer, wait once, then the local inverse transforms and epilogues
-    constexpr int G = cluster_group<N, C>();
     std::uint32_t pw[EW];
     if (pid) {
 #pragma unroll
@@ -414,7 +413,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
           const int k = kspec<N, C, NT>(j, t, c);
           v[j] = pmul(S[rf::pad(t + j * NT)], m[k], m[N + k]);
         }
-        inverse_send<N, C, NT>(v, ex, q, xi, t, c);
+        inverse_send<N, C, NT, G>(v, ex, q, xi, t, c);
       }
       xwait(ex);
 #pragma unroll 1
@@ -471,7 +470,7 @@ __device__ __forceinline__ void step(cf (&v)[Shape<N, C, NT>::E], cf* S, cf (&ou
 
 // Persistent cluster kernel: each cluster pulls work items from `queue` (rank 0 takes the next
 // index and shares it through distributed shared memory).
-template <int N, int C, int NT, class RADS>
+template <int N, int C, int NT, class RADS, int G = r2c::cluster_group<N, C>()>
 __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
     k_resident2d_cluster(const R2Item* __restrict__ items, int nitems, int* queue,
                          const Tw<float>* __restrict__ tw_global) {
@@ -493,9 +492,9 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   const Tw<float>* xg = tw_global + (S::M - 1);
   const Tw<float>* xf = xg + c * S::M;   // forward: this CTA's c, every k1
   const Tw<float>* xi = xg + c * S::MB;  // inverse: entry d·M + k1l for k1 = c·MB + k1l
-  float* mask_s = reinterpret_cast<float*>(smem_raw + r2c::cluster_lines_bytes<N, C>());
-  if constexpr (r2c::cluster_xtw_in_smem<N, C>()) {  // read first after the cluster barrier below
-    Tw<float>* xfs = reinterpret_cast<Tw<float>*>(smem_raw + r2c::cluster_mask_end<N, C>());
+  float* mask_s = reinterpret_cast<float*>(smem_raw + r2c::cluster_lines_bytes<N, C, G>());
+  if constexpr (r2c::cluster_xtw_in_smem<N, C, G>()) {  // read first after the cluster barrier below
+    Tw<float>* xfs = reinterpret_cast<Tw<float>*>(smem_raw + r2c::cluster_mask_end<N, C, G>());
     Tw<float>* xis = xfs + S::M;
     for (int i = t; i < S::M; i += NT) {
       xfs[i] = xf[i];
@@ -506,7 +505,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
   }
   r2c::Exchange ex;
   ex.buf[0] = Sl + rf::padded(S::M);
-  ex.buf[1] = ex.buf[0] + r2c::cluster_group<N, C>() * S::M;
+  ex.buf[1] = ex.buf[0] + G * S::M;
   ex.mbar[0] = r2c::smem_u32(&s_mbar[0]);
   ex.mbar[1] = r2c::smem_u32(&s_mbar[1]);
   ex.parity = 0;
@@ -571,7 +570,7 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(NT, 1)
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        r2c::step<N, C, NT, RADS>(v, Sl, out, b0, b1, phase, ex, it, st, p0, p1, nx, next_p,
+        r2c::step<N, C, NT, RADS, G>(v, Sl, out, b0, b1, phase, ex, it, st, p0, p1, nx, next_p,
                                   next_backward, backward, reflect, store, add, mk, tw, xf, xi, t,
                                   c);
       }

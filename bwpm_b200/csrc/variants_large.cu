@@ -13,11 +13,15 @@ FixedVariant fixed() {
   return {N, NT, 1, {R...}, (const void*)k_resident2d_fixed<N, NT, Radices<R...>>, fixed_smem_bytes<N>()};
 }
 
-// one line over a cluster of C CTAs
+// one line over a cluster of C CTAs, G passes per inverse exchange
+template <int N, int C, int NT, int G, int... R>
+FixedVariant cluster_g() {
+  return {N, NT, C, {R...}, (const void*)k_resident2d_cluster<N, C, NT, Radices<R...>, G>,
+          r2c::cluster_smem_bytes<N, C, G>()};
+}
 template <int N, int C, int NT, int... R>
 FixedVariant cluster() {
-  return {N, NT, C, {R...}, (const void*)k_resident2d_cluster<N, C, NT, Radices<R...>>,
-          r2c::cluster_smem_bytes<N, C>()};
+  return cluster_g<N, C, NT, r2c::cluster_group<N, C>(), R...>();
 }
 }  // namespace
 
