@@ -147,23 +147,29 @@ __device__ __forceinline__ double flux(const cf (&v)[E], const double* w, double
   return total;
 }
 
-// One slab step (cf. r2f_step: prefetched records and operator values; mk: the item's mask in
-// shared memory, n hi then n lo values, or null); every thread of the block calls it.
+// One slab step (cf. r2f_step: prefetched records and operator values, pair ids of the owned
+// pixels once per step, the next pass's operator values prefetched into L1, the first interface
+// round loaded before the forward transform; mk: the item's mask in shared memory, n hi then n lo
+// values, or null); every thread of the block calls it.
 template <int E>
 __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf* b1, int& phase,
                                      const R2Item& it, const R2Step& st, const R2Pass& p0,
-                                     R2Next& nx, int next_p, bool next_backward, bool backward,
-                                     bool reflect, cf* store, const cf* add, const float* mk,
-                                     const FftPlan& plan, const Tw<float>* __restrict__ tw, int t,
-                                     int nt) {
+                                     const R2Pass& p1, R2Next& nx, int next_p, bool next_backward,
+                                     bool backward, bool reflect, cf* store, const cf* add,
+                                     const float* mk, const FftPlan& plan,
+                                     const Tw<float>* __restrict__ tw, int t, int nt) {
+  constexpr int EW = (E + 3) / 4;
   const int n = it.n, nthr = static_cast<int>(blockDim.x);
   const bool own = t < nt;
   const int off = backward ? st.bwd_off : st.fwd_off;
-  const int ntp = backward ? st.bwd_t : st.fwd_t;
-  const int npass = ntp + (reflect ? (backward ? st.bwd_r : st.fwd_r) : 0);
+  const int npass = r2_passes(st, backward, reflect);
   const std::uint8_t* pid = st.pid >= 0 ? it.pids + st.pid : nullptr;
   const int* iface = it.iface + st.iface;
   if (next_p >= 0) nx.st = it.steps[next_p];
+  // interface entry t, the first round of the gather and add loops
+  const bool own_if = t < st.niface;
+  const int q0 = own_if ? iface[t] : 0;
+  const cf a0 = (add && own_if) ? add[t] : cf{0.f, 0.f};
   if (npass == 1) {
     const cf* m = it.tables + p0.tab;
     cf th[E], tl[E];  // in flight during the forward transform
@@ -175,7 +181,7 @@ __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf
       }
     }
     fft<-1, E>(v, b0, b1, phase, plan, tw, t, nt);
-    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (next_p >= 0) r2_next_passes(nx, it, next_backward);
     if (own) {
 #pragma unroll
       for (int k = 0; k < E; ++k) v[k] = pmul(v[k], th[k], tl[k]);
@@ -189,15 +195,41 @@ __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf
       }
     }
   } else {
+    std::uint32_t pw[EW];
+#pragma unroll
+    for (int w = 0; w < EW; ++w) pw[w] = 0;
+    if (pid && own) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) pw[k >> 2] |= static_cast<std::uint32_t>(pid[t + k * nt]) << (8 * (k & 3));
+    }
+    if (own) {
+      const cf* m = it.tables + p0.tab;
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        prefetch_l1(m + t + k * nt);
+        prefetch_l1(m + n + t + k * nt);
+      }
+    }
     fft<-1, E>(v, b0, b1, phase, plan, tw, t, nt);
-    if (next_p >= 0) nx.p0 = it.passes[next_backward ? nx.st.bwd_off : nx.st.fwd_off];
+    if (next_p >= 0) r2_next_passes(nx, it, next_backward);
+    const int pid0 = (pid && own_if) ? pid[q0] : 0;
     if (own) {
 #pragma unroll
       for (int k = 0; k < E; ++k) S[rf::pad(t + k * nt)] = v[k];
     }
+    R2Pass cur = p0, nxt = p1;
     for (int j = 0; j < npass; ++j) {
-      const R2Pass ps = j == 0 ? p0 : it.passes[off + j];
-      const cf* m = it.tables + ps.tab;
+      R2Pass nn = cur;
+      if (j + 2 < npass) nn = it.passes[off + j + 2];
+      if (own && j + 1 < npass) {
+        const cf* mn = it.tables + nxt.tab;
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+          prefetch_l1(mn + t + k * nt);
+          prefetch_l1(mn + n + t + k * nt);
+        }
+      }
+      const cf* m = it.tables + cur.tab;
       if (own) {
 #pragma unroll
         for (int k = 0; k < E; ++k) {
@@ -207,12 +239,12 @@ __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf
         }
       }
       fft<+1, E>(v, b0, b1, phase, plan, tw, t, nt);
-      if (!ps.refl) {
+      if (!cur.refl) {
         if (own) {
 #pragma unroll
           for (int k = 0; k < E; ++k) {
             const int q = t + k * nt;
-            if (!pid || pid[q] == ps.pair) out[k] = mk ? mask_mul(v[k], mk[q], mk[n + q]) : v[k];
+            if (!pid || unpack_pid<E>(pw, k) == cur.pair) out[k] = mk ? mask_mul(v[k], mk[q], mk[n + q]) : v[k];
             if ((k & 3) == 3) asm volatile("" ::: "memory");
           }
         }
@@ -223,12 +255,15 @@ __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf
           for (int k = 0; k < E; ++k) buf[rf::pad(t + k * nt)] = v[k];
         }
         __syncthreads();
-        for (int k = t; k < st.niface; k += nthr) {
+        if (own_if && (!pid || pid0 == cur.pair)) store[t] = buf[rf::pad(q0)];
+        for (int k = t + nthr; k < st.niface; k += nthr) {
           const int q = iface[k];
-          if (!pid || pid[q] == ps.pair) store[k] = buf[rf::pad(q)];
+          if (!pid || pid[q] == cur.pair) store[k] = buf[rf::pad(q)];
         }
         phase ^= 1;
       }
+      cur = nxt;
+      nxt = nn;
     }
     if (own) {
 #pragma unroll
@@ -242,7 +277,11 @@ __device__ __forceinline__ void step(cf (&v)[E], cf* S, cf (&out)[E], cf* b0, cf
       for (int k = 0; k < E; ++k) buf[rf::pad(t + k * nt)] = v[k];
     }
     __syncthreads();
-    for (int k = t; k < st.niface; k += nthr) {
+    if (own_if) {
+      const int q = rf::pad(q0);
+      buf[q] = buf[q] + a0;
+    }
+    for (int k = t + nthr; k < st.niface; k += nthr) {
       const int q = rf::pad(iface[k]);
       buf[q] = buf[q] + add[k];
     }
@@ -319,7 +358,7 @@ __global__ void __launch_bounds__(rg::rt_max_threads(E), 1)
     const int sweeps = it.iterations > 0 ? 2 * it.iterations : 1;
     R2Next nx;
     nx.st = it.steps[0];
-    nx.p0 = it.passes[nx.st.fwd_off];
+    r2_next_passes(nx, it, false);
     for (int sw = 0; sw < sweeps; ++sw) {
       const bool backward = sw & 1;
       const int iter = sw >> 1;
@@ -330,15 +369,15 @@ __global__ void __launch_bounds__(rg::rt_max_threads(E), 1)
       for (int s = 0; s < it.nz; ++s) {
         const int p = backward ? it.nz - 1 - s : s;
         const R2Step st = nx.st;
-        const R2Pass p0 = nx.p0;
+        const R2Pass p0 = nx.p0, p1 = nx.p1;
         bool next_backward;
         const int next_p = next_step(s, p, it.nz, sw, sweeps, backward, next_backward);
-        const bool reflect = st.niface > 0 && (backward || it.iterations > 0);
+        const bool reflect = r2_reflects(st, backward, it.iterations);
         const bool has_add = st.niface > 0 && (backward || iter > 0);
         cf* store = (backward ? it.src_fwd : it.src_bwd) + st.iface;
         const cf* add = has_add ? (backward ? it.src_bwd : it.src_fwd) + st.iface : nullptr;
-        rg::step<E>(v, S, out, b0, b1, phase, it, st, p0, nx, next_p, next_backward, backward,
-                    reflect, store, add, mk, plan, tws, t, nt);
+        rg::step<E>(v, S, out, b0, b1, phase, it, st, p0, p1, nx, next_p, next_backward,
+                    backward, reflect, store, add, mk, plan, tws, t, nt);
       }
       cf* dst = backward ? it.reflected : it.transmitted;
       if (own) {
