@@ -41,9 +41,9 @@ REDUCED: dict = {}  # set by --reduced (profiling runs); empty for the benchmark
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs × FP32 lanes × FMA × max clock
 # DRAM bytes (read + write) of the class kernels of one batched run of this workload, summed
 # over the classes, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, kernel
-# variants of the autotuner); the fields stay on chip, this is operator tables and pair ids L2
-# cannot hold
-TRAFFIC_PER_RUN_BYTES = 1.72e9
+# variants of the autotuner); the fields stay on chip, this is mostly pair-id planes of the
+# longest lines that L2 cannot hold
+TRAFFIC_PER_RUN_BYTES = 1.82e9
 
 
 def _dist():
