@@ -183,6 +183,47 @@ def test_every_kernel_variant_matches_fp64(n):
         assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64, (n, k, cls[0])
 
 
+def _seven_pass_problem(n, pol):
+    """Three dielectrics behind two parallel tilted faces that cross the line on every slab: each
+    step has 5 transmission passes (air, glass, n = 2 and the two interfaces) and 2 reflection
+    passes, more than one group of passes per exchange in every cluster kernel."""
+    from bwpm_b200.workloads import Problem, _vec, absorbing_mask_1d, centred, k0_of
+
+    wl, nz, tilt, theta = 0.55, 40, 0.1, 0.15
+    lam = wl * 1e-3
+    dy, dz, k0 = lam / 8, lam / 10, k0_of(wl)
+    y = centred(n, dy)
+    z = (np.arange(nz) + 0.5) * dz
+    front = 10 * dz + np.tan(tilt) * y
+    back = front + 10 * dz
+    labels = ((z[:, None] >= front[None, :]).astype(np.int32) +
+              (z[:, None] >= back[None, :]).astype(np.int32))[:, :, None]
+    w0 = n * dy / 8
+    prof = (np.exp(-((y / w0) ** 2)) * np.exp(1j * k0 * np.sin(theta) * y))[:, None]
+    mask = absorbing_mask_1d(y, n * dy / 10)[:, None]
+    return Problem(n, 1, dy, 1.0, dz, k0, np.array([1.0 + 0j, 1.5 + 0j, 2.0 + 0j]), labels,
+                   1.0 + 0j, mask, _vec(prof, pol), 2, name=f"seven_pass_{n}_{pol}")
+
+
+@pytest.mark.parametrize("n", (4096, 6144, 8192))
+def test_cluster_variants_on_steps_with_more_passes_than_a_group(n):
+    """Steps with 7 passes: the inverse transforms go out in several groups (4 + 3 or 2 + 2 + 2 + 1
+    per exchange); every variant of the length against FP64, TE and TM."""
+    from bwpm_b200.batch import Batch2D, variant_count
+
+    for pol in ("te", "tm"):
+        p = _seven_pass_problem(n, pol)
+        ref = _fp64(p)
+        for k in range(variant_count(n)):
+            b = Batch2D()
+            b.set_variant(n, k)
+            i = b.add_problem(p)
+            b.run()
+            r = b.result(i)
+            assert rel_l2(r["transmitted"], ref["transmitted"][:, 0]) < L2_C64, (n, pol, k)
+            assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64, (n, pol, k)
+
+
 def test_autotuned_batch_equals_forced_variant():
     """Autotuning picks a variant per length; the results equal a run forced to that variant."""
     from bwpm_b200 import workloads
