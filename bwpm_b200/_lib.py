@@ -60,6 +60,10 @@ SIGNATURES: dict[str, tuple] = {
                                    _i64p]),
     "bwpm_server_submit_3d": (_i, [_p, _sz, _sz, _d, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _p,
                                    _i, _i64p]),
+    "bwpm_server_submit_2d_borrowed": (_i, [_p, _sz, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _p,
+                                            _i, _i64p]),
+    "bwpm_server_submit_3d_borrowed": (_i, [_p, _sz, _sz, _d, _d, _d, _d, _p, _sz, _p, _sz, _d, _d,
+                                            _p, _p, _i, _i64p]),
     "bwpm_server_wait": (_i, [_p, ctypes.c_int64, _d, ctypes.POINTER(_i)]),
     "bwpm_server_result": (_i, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, _p, _p, _p]),
     "bwpm_server_stats": (_i, [_p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),

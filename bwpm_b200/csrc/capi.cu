@@ -49,6 +49,58 @@ bwpm::cd* as_cd(double* p) { return reinterpret_cast<bwpm::cd*>(p); }
 
 }  // namespace
 
+namespace {
+// borrow: the labels stay caller-owned and are copied by a preparation worker of the server
+int server_submit_2d(bwpm_server* s, size_t ny, double dy, double dz, double k0,
+                     const double* indices, size_t m, const int32_t* labels, size_t nz,
+                     double ib_re, double ib_im, const double* mask, const double* field,
+                     int iterations, int64_t* ticket, bool borrow) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
+    bwpm::Solve2D p;
+    p.ny = static_cast<int>(ny);
+    p.nz = static_cast<int>(nz);
+    p.dy = dy;
+    p.dz = dz;
+    p.k0 = k0;
+    p.indices.assign(as_cd(indices), as_cd(indices) + m);
+    if (!borrow) p.labels.assign(labels, labels + nz * ny);
+    p.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) p.mask.assign(mask, mask + ny);
+    p.field.assign(as_cd(field), as_cd(field) + 2 * ny);
+    p.iterations = iterations;
+    const int64_t k = s->impl->submit2d(std::move(p), borrow ? labels : nullptr);
+    if (ticket) *ticket = k;
+  });
+}
+
+int server_submit_3d(bwpm_server* s, size_t ny, size_t nx, double dy, double dx, double dz,
+                     double k0, const double* indices, size_t m, const int32_t* labels,
+                     size_t nz, double ib_re, double ib_im, const double* mask,
+                     const double* field, int iterations, int64_t* ticket, bool borrow) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
+    bwpm::SolverInput in;
+    in.ny = ny;
+    in.nx = nx;
+    in.dy = dy;
+    in.dx = dx;
+    in.dz = dz;
+    in.k0 = k0;
+    in.indices.assign(as_cd(indices), as_cd(indices) + m);
+    if (!borrow) in.labels.assign(labels, labels + nz * ny * nx);
+    in.nz = nz;
+    in.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) in.mask.assign(mask, mask + ny * nx);
+    std::vector<bwpm::cd> f(as_cd(field), as_cd(field) + 2 * ny * nx);
+    const int64_t k = s->impl->submit3d(std::move(in), std::move(f), iterations, borrow ? labels : nullptr);
+    if (ticket) *ticket = k;
+  });
+}
+}  // namespace
+
 extern "C" {
 
 size_t bwpm_last_error(char* buf, size_t len) {
@@ -296,53 +348,38 @@ int bwpm_server_create(int device, uint64_t budget_bytes, int max_groups, int ma
   });
 }
 
+
 int bwpm_server_submit_2d(bwpm_server* s, size_t ny, double dy, double dz, double k0,
                           const double* indices, size_t m, const int32_t* labels, size_t nz,
                           double ib_re, double ib_im, const double* mask, const double* field,
                           int iterations, int64_t* ticket) {
-  return guarded([&] {
-    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
-    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
-    bwpm::Solve2D p;
-    p.ny = static_cast<int>(ny);
-    p.nz = static_cast<int>(nz);
-    p.dy = dy;
-    p.dz = dz;
-    p.k0 = k0;
-    p.indices.assign(as_cd(indices), as_cd(indices) + m);
-    p.labels.assign(labels, labels + nz * ny);
-    p.index_before = bwpm::cd{ib_re, ib_im};
-    if (mask) p.mask.assign(mask, mask + ny);
-    p.field.assign(as_cd(field), as_cd(field) + 2 * ny);
-    p.iterations = iterations;
-    const int64_t k = s->impl->submit2d(std::move(p));
-    if (ticket) *ticket = k;
-  });
+  return server_submit_2d(s, ny, dy, dz, k0, indices, m, labels, nz, ib_re, ib_im, mask, field,
+                          iterations, ticket, false);
+}
+
+int bwpm_server_submit_2d_borrowed(bwpm_server* s, size_t ny, double dy, double dz, double k0,
+                                   const double* indices, size_t m, const int32_t* labels,
+                                   size_t nz, double ib_re, double ib_im, const double* mask,
+                                   const double* field, int iterations, int64_t* ticket) {
+  return server_submit_2d(s, ny, dy, dz, k0, indices, m, labels, nz, ib_re, ib_im, mask, field,
+                          iterations, ticket, true);
 }
 
 int bwpm_server_submit_3d(bwpm_server* s, size_t ny, size_t nx, double dy, double dx, double dz,
                           double k0, const double* indices, size_t m, const int32_t* labels,
                           size_t nz, double ib_re, double ib_im, const double* mask,
                           const double* field, int iterations, int64_t* ticket) {
-  return guarded([&] {
-    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
-    if (!indices || !labels || !field) throw bwpm::invalid_argument("null array");
-    bwpm::SolverInput in;
-    in.ny = ny;
-    in.nx = nx;
-    in.dy = dy;
-    in.dx = dx;
-    in.dz = dz;
-    in.k0 = k0;
-    in.indices.assign(as_cd(indices), as_cd(indices) + m);
-    in.labels.assign(labels, labels + nz * ny * nx);
-    in.nz = nz;
-    in.index_before = bwpm::cd{ib_re, ib_im};
-    if (mask) in.mask.assign(mask, mask + ny * nx);
-    std::vector<bwpm::cd> f(as_cd(field), as_cd(field) + 2 * ny * nx);
-    const int64_t k = s->impl->submit3d(std::move(in), std::move(f), iterations);
-    if (ticket) *ticket = k;
-  });
+  return server_submit_3d(s, ny, nx, dy, dx, dz, k0, indices, m, labels, nz, ib_re, ib_im, mask,
+                          field, iterations, ticket, false);
+}
+
+int bwpm_server_submit_3d_borrowed(bwpm_server* s, size_t ny, size_t nx, double dy, double dx,
+                                   double dz, double k0, const double* indices, size_t m,
+                                   const int32_t* labels, size_t nz, double ib_re, double ib_im,
+                                   const double* mask, const double* field, int iterations,
+                                   int64_t* ticket) {
+  return server_submit_3d(s, ny, nx, dy, dx, dz, k0, indices, m, labels, nz, ib_re, ib_im, mask,
+                          field, iterations, ticket, true);
 }
 
 int bwpm_server_wait(bwpm_server* s, int64_t ticket, double timeout_s, int* done) {

@@ -156,11 +156,21 @@ template <typename T>
 void PlaneSolver<T>::setup() {
   const std::size_t nn = n();
   if (in_.ny < 1 || in_.nx < 1) throw invalid_argument("ny and nx must be positive");
-  if (in_.labels.size() != in_.nz * nn) throw invalid_argument("labels must have shape (nz, ny, nx)");
+  const std::int32_t* labels = in_.labels_view ? in_.labels_view : in_.labels.data();
+  if (!in_.labels_view && in_.labels.size() != in_.nz * nn)
+    throw invalid_argument("labels must have shape (nz, ny, nx)");
   if (!in_.mask.empty() && in_.mask.size() != nn) throw invalid_argument("mask must have shape (ny, nx)");
-  for (auto l : in_.labels)
-    if (l < 0 || static_cast<std::size_t>(l) >= in_.indices.size())
+  {  // range check as a min/max reduction (vectorises; one pass over the labels)
+    std::int32_t lo = 0, hi = 0;
+    const std::size_t nl = in_.nz * nn;
+    if (nl > 0) lo = hi = labels[0];
+    for (std::size_t i = 0; i < nl; ++i) {
+      lo = std::min(lo, labels[i]);
+      hi = std::max(hi, labels[i]);
+    }
+    if (lo < 0 || static_cast<std::size_t>(hi) >= in_.indices.size())
       throw invalid_argument("labels must index into `indices`");
+  }
   if (nn > (1u << 30)) throw invalid_argument("plane too large");
   if (in_.indices.size() > 4096) throw invalid_argument("at most 4096 materials");
   // Born hosts per slab (cpp/src/solver.cpp:49-62)
@@ -174,7 +184,7 @@ void PlaneSolver<T>::setup() {
       for (std::size_t q = 0; q < nn; ++q) {
         const cd d = in_.fluct[j * nn + q];
         if (d.re == 0.0 && d.im == 0.0) continue;
-        const cd idx = in_.indices[static_cast<std::size_t>(in_.labels[j * nn + q])];
+        const cd idx = in_.indices[static_cast<std::size_t>(labels[j * nn + q])];
         if (has && (host.re != idx.re || host.im != idx.im))
           throw invalid_argument("slab " + std::to_string(j) + ": fluctuation must lie in one host index");
         has = true;
@@ -221,8 +231,8 @@ void PlaneSolver<T>::setup() {
   std::vector<std::uint32_t> code(nn), stamp(ncode, 0);
   std::vector<int> code_id(ncode, -1);
   for (std::size_t p = 0; p < in_.nz; ++p) {
-    const std::int32_t* a = p == 0 ? before.data() : in_.labels.data() + (p - 1) * nn;
-    const std::int32_t* b = in_.labels.data() + p * nn;
+    const std::int32_t* a = p == 0 ? before.data() : labels + (p - 1) * nn;
+    const std::int32_t* b = labels + p * nn;
     const std::uint32_t mark = static_cast<std::uint32_t>(p) + 1;
     std::vector<std::uint32_t> present;
     for (std::size_t q = 0; q < nn; ++q) {
@@ -282,6 +292,7 @@ void PlaneSolver<T>::setup() {
     }
     max_pass_ = std::max(max_pass_, npass);
   }
+  in_.labels_view = nullptr;  // the caller's labels are not read after set-up
   iface_total_ = static_cast<long long>(iface_host.size());
   if (!pid_host.empty()) {
     pid_pool_.alloc(pid_host.size(), stream_);

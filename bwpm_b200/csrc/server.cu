@@ -40,6 +40,8 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 struct Request {
   std::int64_t id = 0;
   bool is3d = false;
+  const std::int32_t* borrowed = nullptr;  // caller-owned labels (2D: copied in preparation; 3D:
+                                           // read in place by the plane engine's set-up)
   Solve2D s2;
   std::shared_ptr<PreparedSolve> prep;
   SolverInput s3;
@@ -98,17 +100,20 @@ class ServerImpl final : public Server {
     for (auto& t : threads_) t.join();
   }
 
-  std::int64_t submit2d(Solve2D s) override {
+  std::int64_t submit2d(Solve2D s, const std::int32_t* labels) override {
     auto r = std::make_shared<Request>();
     r->s2 = std::move(s);
+    r->borrowed = labels;
     return enqueue(std::move(r));
   }
 
-  std::int64_t submit3d(SolverInput in, std::vector<cd> field, int iterations) override {
+  std::int64_t submit3d(SolverInput in, std::vector<cd> field, int iterations,
+                        const std::int32_t* labels) override {
     if (in.ny * in.nx * 2 != field.size()) throw invalid_argument("field must have shape (ny, nx, 2)");
     if (iterations < 0) throw invalid_argument("iterations must be >= 0");
     auto r = std::make_shared<Request>();
     r->is3d = true;
+    r->borrowed = labels;
     in.device = opt_.device;
     r->s3 = std::move(in);
     r->field3 = std::move(field);
@@ -182,6 +187,13 @@ class ServerImpl final : public Server {
       }
       std::string err;
       try {
+        if (r->borrowed) {  // caller-owned labels: 2D copies them here, on the worker threads;
+          if (r->is3d)      // the 3D set-up reads them in place on its runner thread
+            r->s3.labels_view = r->borrowed;
+          else
+            r->s2.labels.assign(r->borrowed, r->borrowed + static_cast<std::size_t>(r->s2.nz) * r->s2.ny);
+          r->borrowed = nullptr;
+        }
         if (r->is3d) {
           r->bytes = estimate_3d_bytes(r->s3);
         } else {

@@ -39,9 +39,13 @@ class Server {
  public:
   virtual ~Server() = default;  // finishes every submitted request first
   // Thread-safe; return a ticket at once. A request that fails validation or on the device is
-  // marked failed: wait() returns, result() throws its error.
-  virtual std::int64_t submit2d(Solve2D s) = 0;
-  virtual std::int64_t submit3d(SolverInput in, std::vector<cd> field, int iterations) = 0;
+  // marked failed: wait() returns, result() throws its error. With `labels` non-null the
+  // request's labels (nz·ny·nx int32) are taken from there instead of s.labels / in.labels (2D:
+  // copied by a preparation worker; 3D: read in place by the set-up of its plane engine): the
+  // caller keeps them valid and unchanged until wait() has reported the request finished.
+  virtual std::int64_t submit2d(Solve2D s, const std::int32_t* labels = nullptr) = 0;
+  virtual std::int64_t submit3d(SolverInput in, std::vector<cd> field, int iterations,
+                                const std::int32_t* labels = nullptr) = 0;
   // true when the request has finished (done or failed) within timeout_s
   virtual bool wait(std::int64_t ticket, double timeout_s) = 0;
   // results of a finished request (the record is released); throws the request's error

@@ -17,6 +17,9 @@ struct SolverInput {
   double dy = 0, dx = 0, dz = 0, k0 = 0;
   std::vector<cd> indices;
   std::vector<std::int32_t> labels;  // (nz, ny, nx)
+  // or, when set, the caller's labels read in place during set-up (nz·ny·nx values, valid until
+  // the solver has been constructed; `labels` is then empty)
+  const std::int32_t* labels_view = nullptr;
   std::size_t nz = 0;
   cd index_before{1.0, 0.0};
   std::vector<double> mask;          // (ny, nx) or empty

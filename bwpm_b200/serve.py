@@ -33,12 +33,14 @@ class Server:
                                      int(max_group_solves), int(max_3d), ctypes.byref(h)))
         self._h = h
         self._shape: dict[int, tuple[int, int, int, bool]] = {}  # ticket -> (ny, nx, iters, 3d)
+        self._borrowed: dict[int, np.ndarray] = {}  # ticket -> labels the server reads later
 
     def close(self) -> None:
         """Waits for every submitted request, then releases the server."""
         if getattr(self, "_h", None):
             lib.bwpm_server_destroy(self._h)
             self._h = None
+            self._borrowed.clear()
 
     def __del__(self):
         self.close()
@@ -49,8 +51,13 @@ class Server:
     def __exit__(self, *exc):
         self.close()
 
-    def submit(self, prob) -> int:
-        """Submits a `bwpm_b200.workloads.Problem` (nx = 1: 2D, else 3D); returns its ticket."""
+    def submit(self, prob, borrow: bool = True) -> int:
+        """Submits a `bwpm_b200.workloads.Problem` (nx = 1: 2D, else 3D); returns its ticket.
+
+        borrow: the server takes the labels after the call returns (2D: copied by a preparation
+        worker, 3D: read in place by the set-up; the Server holds the array until the request's
+        result is taken), so a large 3D submission does not stall the caller; False copies
+        everything inside the call."""
         labels = np.ascontiguousarray(prob.labels, dtype=np.int32)
         indices = np.ascontiguousarray(prob.indices, dtype=np.complex128).ravel()
         field = np.ascontiguousarray(prob.field, dtype=np.complex128)
@@ -61,15 +68,17 @@ class Server:
         if prob.fluctuation is not None:
             raise ValueError("the server takes problems without a fluctuation term")
         if prob.nx == 1:
-            check(lib.bwpm_server_submit_2d(
-                self._h, prob.ny, prob.dy, prob.dz, prob.k0, ptr(indices), indices.size,
-                ptr(labels), nz, ib.real, ib.imag, ptr(mask), ptr(field), int(prob.iterations),
-                ctypes.byref(t)))
+            fn = lib.bwpm_server_submit_2d_borrowed if borrow else lib.bwpm_server_submit_2d
+            check(fn(self._h, prob.ny, prob.dy, prob.dz, prob.k0, ptr(indices), indices.size,
+                     ptr(labels), nz, ib.real, ib.imag, ptr(mask), ptr(field),
+                     int(prob.iterations), ctypes.byref(t)))
         else:
-            check(lib.bwpm_server_submit_3d(
-                self._h, prob.ny, prob.nx, prob.dy, prob.dx, prob.dz, prob.k0, ptr(indices),
-                indices.size, ptr(labels), nz, ib.real, ib.imag, ptr(mask), ptr(field),
-                int(prob.iterations), ctypes.byref(t)))
+            fn = lib.bwpm_server_submit_3d_borrowed if borrow else lib.bwpm_server_submit_3d
+            check(fn(self._h, prob.ny, prob.nx, prob.dy, prob.dx, prob.dz, prob.k0, ptr(indices),
+                     indices.size, ptr(labels), nz, ib.real, ib.imag, ptr(mask), ptr(field),
+                     int(prob.iterations), ctypes.byref(t)))
+        if borrow:
+            self._borrowed[t.value] = labels
         self._shape[t.value] = (prob.ny, prob.nx, int(prob.iterations), prob.nx != 1)
         return int(t.value)
 
@@ -81,6 +90,7 @@ class Server:
     def result(self, ticket: int) -> dict:
         """Waits for the request and returns its results (the ticket is released)."""
         self.wait(ticket)
+        self._borrowed.pop(ticket, None)  # finished: the server no longer reads the labels
         ny, nx, iters, is3d = self._shape.pop(ticket)
         t = np.empty((ny, nx, 2), dtype=np.complex128)
         r = np.empty((ny, nx, 2), dtype=np.complex128)

@@ -165,6 +165,23 @@ int bwpm_server_submit_3d(bwpm_server* s, size_t ny, size_t nx, double dy, doubl
                           const double* mask, const double* field, int iterations,
                           int64_t* ticket);
 
+/* The two submissions above with borrowed labels: the call copies only the small arrays and
+ * returns; the server takes the labels later (2D: a preparation worker copies the nz·ny values;
+ * 3D: the request's set-up reads the nz·ny·nx values in place), so the caller keeps `labels`
+ * valid and unchanged until bwpm_server_wait reports the request finished. Submitting large 3D
+ * requests then costs the submitting thread no copy. No reference counterpart (the served loop
+ * is new). */
+int bwpm_server_submit_2d_borrowed(bwpm_server* s, size_t ny, double dy, double dz, double k0,
+                                   const double* indices, size_t m, const int32_t* labels,
+                                   size_t nz, double index_before_re, double index_before_im,
+                                   const double* mask, const double* field, int iterations,
+                                   int64_t* ticket);
+int bwpm_server_submit_3d_borrowed(bwpm_server* s, size_t ny, size_t nx, double dy, double dx,
+                                   double dz, double k0, const double* indices, size_t m,
+                                   const int32_t* labels, size_t nz, double index_before_re,
+                                   double index_before_im, const double* mask,
+                                   const double* field, int iterations, int64_t* ticket);
+
 /* Waits up to timeout_s seconds (< 0: without limit); *done = 1 when the request finished. */
 int bwpm_server_wait(bwpm_server* s, int64_t ticket, double timeout_s, int* done);
 

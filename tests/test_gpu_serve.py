@@ -106,3 +106,24 @@ def test_served_failed_request_does_not_stop_the_others():
             assert np.array_equal(srv.result(t)["transmitted"], _alone_2d(p)["transmitted"])
         st = srv.stats()
     assert st["failed"] == 1 and st["completed"] == 3
+
+
+def test_borrowed_and_copied_submissions_give_the_same_results():
+    """Borrowed labels (copied later by the server's preparation workers) and labels copied in
+    the call give the same results, 2D and 3D, and the caller's own array may go away at once."""
+    from bwpm_b200.serve import Server
+
+    probs = _stream()[:6]
+    with Server() as srv:
+        copied = [srv.result(srv.submit(p, borrow=False)) for p in probs]
+    with Server() as srv:
+        tickets = []
+        for p in probs:
+            # a private copy that only the Server keeps alive after the call
+            q = type(p)(**{**p.__dict__, "labels": np.array(p.labels, copy=True)})
+            tickets.append(srv.submit(q))
+            del q
+        borrowed = [srv.result(t) for t in tickets]
+    for p, a, b in zip(probs, copied, borrowed):
+        assert np.array_equal(a["transmitted"], b["transmitted"]), p.name
+        assert np.array_equal(a["reflected"], b["reflected"]), p.name
