@@ -16,7 +16,7 @@ struct ServerOptions {
   std::size_t budget_bytes = 0;  // device memory for requests in flight; 0: 80 % of free memory
   int max_groups = 8;            // 2D launch groups in flight
   int max_group_solves = 64;     // solves per 2D launch group
-  int max_3d = 8;                // 3D solves in flight
+  int max_3d = 16;               // 3D solves in flight (each runner also does its host set-up)
   int prep_threads = 0;          // host preparation workers; 0: one per host core, at most 16
 };
 

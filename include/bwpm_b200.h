@@ -144,7 +144,7 @@ void bwpm_batch_destroy(bwpm_batch* b);
  * arrival order while the device-memory budget holds, and launched in groups on the batched
  * resident engine; groups launched while others run share the GPU. 3D requests run through the
  * complex64 plane engine on their own streams. budget_bytes 0: 80 % of the free device memory;
- * max_groups / max_group_solves / max_3d ≤ 0: defaults (8, 64, 8). Destroying the server waits
+ * max_groups / max_group_solves / max_3d ≤ 0: defaults (8, 64, 16). Destroying the server waits
  * for every submitted request. */
 typedef struct bwpm_server bwpm_server;
 
