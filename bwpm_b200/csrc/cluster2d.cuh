@@ -63,7 +63,8 @@ __host__ __device__ constexpr int cluster_group() {
     if (cluster_base_bytes<N, C>(g) <= kClusterSmemCap) return g;
   return 1;
 }
-// (a variant may take a smaller G, so that two CTAs fit on one SM)
+// layout for a given G (the kernel's template parameter; the variant registry takes
+// cluster_group's choice)
 template <int N, int C, int G>
 __host__ __device__ constexpr std::size_t cluster_lines_bytes() {
   return (static_cast<std::size_t>(3 * rf::padded(N / C) + 2 * G * (N / C)) * sizeof(cf) + 15) / 16 * 16;
