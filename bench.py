@@ -73,31 +73,42 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_ms: int = 100):
         self.device = device
+        self.period_ms = period_ms
         self.rows: list[list[str]] = []
-        self._stop = threading.Event()
-        self._t = threading.Thread(target=self._loop, daemon=True)
+        self._p = None
+        self._t = None
 
-    def _loop(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
-            except Exception:  # noqa: BLE001 - sampling is best effort
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._p.stdout:
+            line = line.strip()
+            if line:
+                self.rows.append([c.strip() for c in line.split(",")])
 
     def __enter__(self):
-        self._t.start()
+        # one nvidia-smi streaming a sample every period_ms (a process per sample would take
+        # longer than the sampling period itself)
+        try:
+            self._p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:  # noqa: BLE001 - sampling is best effort (no nvidia-smi: no samples)
+            self._p = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is not None:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._p.kill()
+        if self._t is not None:
+            self._t.join(timeout=5)
 
     def summary(self) -> dict:
         if not self.rows:
@@ -529,7 +540,7 @@ def _peak(key: str) -> float:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp64-sample", type=int, default=6)
