@@ -11,7 +11,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import load_golden, load_npz, rel_l2
+from conftest import load_npz, rel_l2
 from golden_cases import case_2d
 
 pytestmark = pytest.mark.gpu
