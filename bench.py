@@ -96,6 +96,9 @@ class Clocks:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            t0 = time.perf_counter()  # the sampler is live before the timed region starts
+            while not self.rows and self._p.poll() is None and time.perf_counter() - t0 < 2.0:
+                time.sleep(0.01)
         except Exception:  # noqa: BLE001 - sampling is best effort (no nvidia-smi: no samples)
             self._p = None
         return self
