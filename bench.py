@@ -128,21 +128,31 @@ class Clocks:
 
 # ---- CPU reference (oracle/_ref: the reference's own C++ CPU core) ---------------------------
 
+_CPU_CORE = None
+
+
+def _ref_kind() -> str:
+    return "reference" if sorted((ROOT / "oracle" / "_ref").glob("_core*.so")) else "port"
+
+
 def _cpu_solve(args):
-    """One solve on the reference CPU core (1 thread) or, without it, the numpy oracle port."""
+    """One solve on the reference CPU core (1 thread) or, without it, the numpy oracle port;
+    returns the solve's own time in s."""
+    global _CPU_CORE
     prm, kind = args
     from bwpm_b200 import workloads
 
     p = workloads.tilted_slab2d_from(prm)
-    t0 = time.perf_counter()
-    if kind == "reference":
+    if kind == "reference" and _CPU_CORE is None:
         import importlib.util
 
         so = sorted((ROOT / "oracle" / "_ref").glob("_core*.so"))[0]
         spec = importlib.util.spec_from_file_location("_core", so)
-        core = importlib.util.module_from_spec(spec)
-        spec.loader.exec_module(core)
-        core.Solver(*p.core_args(), 1).run(p.field, p.iterations, [])
+        _CPU_CORE = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(_CPU_CORE)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        _CPU_CORE.Solver(*p.core_args(), 1).run(p.field, p.iterations, [])
     else:
         from oracle import port
 
@@ -150,62 +160,114 @@ def _cpu_solve(args):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(params: list[dict], budget_s: float = 20.0) -> dict:
-    """Reference CPU throughput on a bounded seeded sample of the batch, all host cores.
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
-    Runs a seeded random sample of the batch's instances as single-threaded solves in a pool of
-    one process per core (no GPU work meanwhile) and reports cores × solves / Σ solve time."""
-    import multiprocessing as mp
 
-    kind = "reference" if sorted((ROOT / "oracle" / "_ref").glob("_core*.so")) else "port"
-    cores = os.cpu_count() or 1
-    rng = np.random.default_rng(123)
-    order = rng.permutation(len(params))
-    # estimated single-thread cost: ≈ 1.2e-8 s per point·log2(N) per slab-pass (reference core)
-    est = [1.2e-8 * p["ny"] * np.log2(p["ny"]) * p["nz"] * 2 * p["iterations"] * 2 for p in params]
-    sample, tot = [], 0.0
-    for i in order:
-        if tot > budget_s * cores and len(sample) >= min(cores, 4):
-            break
-        sample.append(int(i))
-        tot += est[i]
-        if len(sample) >= 4 * cores:
-            break
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(min(cores, len(sample))) as pool:
-        times = pool.map(_cpu_solve, [(params[i], kind) for i in sample])
-    wall = time.perf_counter() - t0
-    per_solve = float(np.mean(times))
-    return {"value": cores / per_solve, "unit": "solves/s", "cores": cores, "kind": kind,
-            "sample": f"{len(sample)} seeded random instances of the batch (indices {sample[:8]}...), "
-                      f"1 thread each in {min(cores, len(sample))} processes; "
-                      f"throughput = cores / mean solve time ({per_solve:.2f} s); wall {wall:.1f} s"}
+def _cost(prm: dict) -> float:
+    """Estimated single-thread cost of one solve: ∝ N·log2 N per slab-pass."""
+    return prm["ny"] * np.log2(prm["ny"]) * prm["nz"] * 2 * max(prm["iterations"], 1)
+
+
+class CpuReference:
+    """The reference CPU implementation on the host cores: one single-threaded solve per core
+    (a process pool, spawned before any GPU work of this process), timed by the wall clock.
+
+    `step(k)` solves slice k of a seeded permutation of the batch (`per_step` instances, longest
+    first, slices rotate over the whole batch) and returns (solves, wall seconds)."""
+
+    def __init__(self, params: list[dict], per_step: int | None = None):
+        import multiprocessing as mp
+
+        self.params = params
+        self.kind = _ref_kind()
+        self.cores = os.cpu_count() or 1
+        self.per_step = per_step or 3 * self.cores
+        self.order = [int(i) for i in np.random.default_rng(123).permutation(len(params))]
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+
+    def warm(self) -> None:
+        """Loads the core in every worker (one small solve each)."""
+        small = min(self.params, key=_cost)
+        self.pool.map(_cpu_solve, [(small, self.kind)] * self.cores, chunksize=1)
+
+    def slice(self, k: int) -> list[int]:
+        n = len(self.order)
+        idx = [self.order[(k * self.per_step + j) % n] for j in range(self.per_step)]
+        return sorted(idx, key=lambda i: -_cost(self.params[i]))
+
+    def step(self, k: int) -> tuple[int, float]:
+        jobs = [(self.params[i], self.kind) for i in self.slice(k)]
+        t0 = time.perf_counter()
+        for _ in self.pool.imap_unordered(_cpu_solve, jobs, chunksize=1):
+            pass
+        return len(jobs), time.perf_counter() - t0
+
+    def close(self) -> None:
+        self.pool.close()
+        self.pool.join()
+
+    def describe(self, steps: int) -> str:
+        return (f"{steps} steps of {self.per_step} seeded instances each (slices of a seeded "
+                f"permutation of the {len(self.params)}-solve batch, longest first), one "
+                f"single-threaded solve per core in {self.cores} processes on {cpu_model()}; "
+                "value = solves / wall time, both measured")
+
+
+def cpu_baseline(ref: CpuReference, steps: int = 2) -> dict:
+    """Reference CPU throughput on a bounded sample of the batch, all host cores."""
+    ref.warm()
+    done, wall = 0, 0.0
+    for k in range(steps):
+        n, w = ref.step(k)
+        done += n
+        wall += w
+    return {"value": done / wall, "unit": "solves/s", "cores": ref.cores, "kind": ref.kind,
+            "cpu": cpu_model(), "sample": ref.describe(steps)}
+
+
+def _config(ws: int, count: int = COUNT) -> dict:
+    """The workload's config, identical in both arms."""
+    return {"workload": WORKLOAD if not REDUCED else f"REDUCED profiling case {REDUCED}",
+            "global_batch": count * ws, "seq_len": None, "parallelism": f"replicas{ws}",
+            "l2": "GPU arm: flushed (512 MB write) before each timed step; CPU arm: n/a"}
 
 
 def run_reference(args) -> None:
+    """The reference arm: the reference's own CPU core (oracle/_ref, built from its sources) on
+    the host cores, each step a measured slice of the workload. Rank 0 alone runs it."""
     dist, rank, ws = _dist_for_reference()
     if rank != 0:
         return
     params = _params()
-    vals = []
-    cb = None
-    for _ in range(args.warmup):
-        pass  # the CPU core has no warm-up state worth a step of its own
-    for _ in range(args.steps):
-        cb = cpu_baseline(params, budget_s=args.cpu_budget)
-        vals.append(cb["value"])
-    v = float(np.median(vals))
+    ref = CpuReference(params, per_step=args.ref_sample or None)
+    ref.warm()
+    for _ in range(args.warmup - 1):  # the first warm-up step loaded the core in every worker
+        ref.warm()
+    done, walls = 0, []
+    for k in range(args.steps):
+        n, w = ref.step(k)
+        done += n
+        walls.append(w)
+    ref.close()
+    v = done / float(np.sum(walls))
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": COUNT / v * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "global_batch": COUNT, "seq_len": None,
-                       "parallelism": "cpu"},
-            "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cb["cores"],
-                             "kind": cb["kind"], "sample": cb["sample"]},
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(walls)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded)", "config": _config(ws, len(params)), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": ref.cores, "kind": ref.kind,
+                             "cpu": cpu_model(), "sample": ref.describe(args.steps)},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "note": f"a step solves {ref.per_step} of the {COUNT} solves (ms_per_step is that "
+                    "slice's measured wall time); value = all solves of the timed steps / their "
+                    "summed wall time"}
     print(json.dumps(line), flush=True)
 
 
@@ -327,15 +389,17 @@ def run_ours(args) -> None:
             configs = run_configs(device)
         except Exception as e:  # noqa: BLE001 - a side measurement must not cost the headline
             configs = {"error": f"{type(e).__name__}: {e}"}
-    cb = cpu_baseline(params, budget_s=args.cpu_budget) if not args.no_cpu else None
+    cb = None
+    if not args.no_cpu:
+        ref = CpuReference(params)
+        cb = cpu_baseline(ref, steps=2)
+        ref.close()
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD if not REDUCED else f"REDUCED profiling case {REDUCED}",
-                   "global_batch": count * ws, "seq_len": None,
-                   "parallelism": f"replicas{ws}", "l2": "flushed (512 MB write) before each timed step",
-                   "work_items": stats["work_items"], "classes": stats["classes"],
+        "config": _config(ws, count),
+        "engine": {"work_items": stats["work_items"], "classes": stats["classes"],
                    "kernels": kernels},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "fp64_plain": {"value": fp64_rate, "unit": "solves/s", "sample": len(sample),
@@ -547,8 +611,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fp64-sample", type=int, default=6)
-    ap.add_argument("--cpu-budget", type=float, default=15.0, help="target CPU seconds per core")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="instances per step of the CPU reference (default: 3 per host core)")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-configs", action="store_true", help="skip configurations 1-3")
     ap.add_argument("--served-fp64", type=int, default=16, help="FP64 sample of the served stream")

@@ -63,6 +63,10 @@ __global__ void k_noalloc_twiddles(Tw<double>* tw, FftPlan plan) {
   tw[i].hi = cd{cs, sn};
 }
 
+// EPT: complex values a thread stages per FFT stage. 16 serves most lengths; lengths whose
+// radix-3/5/7 stages would need more than kNoAllocThreads threads at 16 (7203, 7350, 7560, 7776,
+// 7840, 7875, 7938, 8000, 8064, 8100) run the EPT = 32 instance.
+template <int EPT>
 __global__ void __launch_bounds__(kNoAllocThreads)
     k_noalloc_step2d(unsigned char* scratch, const cd* in, cd* out, const std::int32_t* lab_before,
                      const std::int32_t* lab_after, const double* mask, Materials mat, int n,
@@ -94,7 +98,7 @@ __global__ void __launch_bounds__(kNoAllocThreads)
     if (tid == 0) atomicExch(status, 1);
     return;
   }
-  fft_smem<-1>(buf, plan, tw, 1, tid, nt);
+  fft_smem<-1, EPT>(buf, plan, tw, 1, tid, nt);
   for (int q = tid; q < n; q += nt) spec[q] = buf[q];
   __syncthreads();
   const double inv_n = 1.0 / static_cast<double>(n);
@@ -109,7 +113,7 @@ __global__ void __launch_bounds__(kNoAllocThreads)
       buf[q] = spec[q] * m3[c == 0 ? 0 : 2];
     }
     __syncthreads();
-    fft_smem<+1>(buf, plan, tw, 1, tid, nt);
+    fft_smem<+1, EPT>(buf, plan, tw, 1, tid, nt);
     for (int q = tid; q < n; q += nt) {
       const int lr = lab_before ? lab_before[q] : -1;
       if (lr != r || lab_after[q] != s) continue;
@@ -175,11 +179,11 @@ bool plan_fixed(int n, FftPlan& p) {
   return true;
 }
 
-int threads_fixed(const FftPlan& p) {
+int threads_fixed(const FftPlan& p, int ept) {
   long long need = 32;
   for (int s = 0; s < p.nstages; ++s) {
     const long long total = p.n / p.radix[s];
-    const long long k = kmax_for(p.radix[s], 16);
+    const long long k = kmax_for(p.radix[s], ept);
     need = std::max(need, (total + k - 1) / k);
   }
   return static_cast<int>((need + 31) / 32 * 32);
@@ -203,8 +207,19 @@ void step2d_noalloc(int device, std::size_t ny, double dy, double dz, double k0,
   FftPlan plan;
   if (!plan_fixed(static_cast<int>(ny), plan))
     throw invalid_argument("ny must factor into 2, 3, 5 and 7 for the allocation-free step");
-  const int threads = std::max(64, threads_fixed(plan));
+  const bool wide = threads_fixed(plan, 16) > kNoAllocThreads;
+  const int threads = std::max(64, threads_fixed(plan, wide ? 32 : 16));
   if (threads > kNoAllocThreads) throw invalid_argument("ny too large for the allocation-free step");
+  // the caller's current device is restored on every exit path (the call selects `device`)
+  struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() {
+      if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceGuard() {
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  } guard;
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
   unsigned char* scratch = nullptr;
   {  // set-up once per device, with that device current: the scratch array's device address
@@ -212,9 +227,10 @@ void step2d_noalloc(int device, std::size_t ny, double dy, double dz, double k0,
     if (!g_scratch_ptr[device]) {
       void* ptr = nullptr;
       check_cuda(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress");
-      check_cuda(cudaFuncSetAttribute(k_noalloc_step2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(kNoAllocMaxN * sizeof(cd))),
-                 "cudaFuncSetAttribute");
+      for (const void* k : {(const void*)k_noalloc_step2d<16>, (const void*)k_noalloc_step2d<32>})
+        check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kNoAllocMaxN * sizeof(cd))),
+                   "cudaFuncSetAttribute");
       g_scratch_ptr[device] = ptr;
     }
     scratch = static_cast<unsigned char*>(g_scratch_ptr[device]);
@@ -230,9 +246,14 @@ void step2d_noalloc(int device, std::size_t ny, double dy, double dz, double k0,
     k_noalloc_twiddles<<<ceil_div(plan.ntw, 256), 256, 0, stream>>>(tw, plan);
     check_cuda(cudaGetLastError(), "k_noalloc_twiddles");
   }
-  k_noalloc_step2d<<<2, threads, ny * sizeof(cd), stream>>>(
-      scratch, field_in, field_out, labels_before, labels_after, mask, mat, static_cast<int>(ny),
-      dy, dz, k0, plan);
+  if (wide)
+    k_noalloc_step2d<32><<<2, threads, ny * sizeof(cd), stream>>>(
+        scratch, field_in, field_out, labels_before, labels_after, mask, mat, static_cast<int>(ny),
+        dy, dz, k0, plan);
+  else
+    k_noalloc_step2d<16><<<2, threads, ny * sizeof(cd), stream>>>(
+        scratch, field_in, field_out, labels_before, labels_after, mask, mat, static_cast<int>(ny),
+        dy, dz, k0, plan);
   check_cuda(cudaGetLastError(), "k_noalloc_step2d");
   int status = 0;
   check_cuda(cudaMemcpyAsync(&status, scratch, sizeof(int), cudaMemcpyDeviceToHost, stream), "status");

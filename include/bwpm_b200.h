@@ -213,11 +213,14 @@ int bwpm_flush_l2(int device, size_t bytes);
  * GPU loading this library holds until exit; the array keeps the last call's contents and all
  * calls on a device share it, so calls that overlap on the GPU (other threads or streams) race.
  * The first call on a device looks up the array's address; make that first call before any
- * stream capture. The call waits for its stream before returning.
+ * stream capture. Every call copies a status word back to the host and waits for its stream
+ * before returning. The call makes `device` current and restores the caller's current device
+ * before it returns.
  * Device pointers: field_in/field_out ny·2 complex, labels_before/labels_after ny int32
  * (labels_before NULL: the medium before the volume, index_before), mask ny doubles or NULL.
  * indices: host array of m ≤ 32 complex. Limits: 2 ≤ ny ≤ BWPM_NOALLOC_MAX_N, ny a product of
- * 2, 3, 5 and 7; anything else returns BWPM_EINVAL with a message. stream: a cudaStream_t or
+ * 2, 3, 5 and 7 (every such length is accepted); anything else returns BWPM_EINVAL with a
+ * message, and so does a label outside [0, m) (found on the device). stream: a cudaStream_t or
  * NULL for the default stream. */
 #define BWPM_NOALLOC_MAX_N 8192
 #define BWPM_NOALLOC_SCRATCH_BYTES 393472

@@ -2,10 +2,11 @@
 # Builds the reference CPU core (bwpm._core: Solver, transmission_matrix, reflection_matrix,
 # longitudinal_wavenumber) from the reference sources, unchanged, into oracle/_ref/.
 # Test infrastructure only: the built module is the checker and the timed CPU baseline, never
-# part of the product path. Needs the reference tree (default /root/reference) and pybind11.
+# part of the product path. Needs the reference tree (BWPM_REFERENCE, default: a `reference`
+# directory beside this repository) and pybind11.
 set -euo pipefail
-REF="${BWPM_REFERENCE:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${BWPM_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/cpp/src/solver.cpp" ]; then
   echo "reference sources not found at $REF; skipping oracle/_ref build" >&2

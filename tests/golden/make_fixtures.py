@@ -1,7 +1,8 @@
 """Generates the golden fixtures under tests/golden/ from the reference (run once, here).
 
-Two sources, both read from the reference tree (default /root/reference, override with
-BWPM_REFERENCE); nothing under tests/ reads the reference at run time, only these fixtures:
+Two sources, both read from the reference tree (BWPM_REFERENCE, default: a `reference`
+directory beside this repository); nothing under tests/ reads the reference at run time, only
+these fixtures:
 
 1. The reference's own golden files `reference/<case>.result.json` (format "raytatouille-result",
    written by the reference's tools/export_reference.py from tools/reference_cases.py). Each is
@@ -13,7 +14,8 @@ BWPM_REFERENCE); nothing under tests/ reads the reference at run time, only thes
      through the reference's compiled CPU core `bwpm._core.Solver` (cpp/src/solver.cpp:444-528)
      built by oracle/build_ref.sh.
 
-Usage: python tests/golden/make_fixtures.py
+Usage: python tests/golden/make_fixtures.py          (golden files, random volumes, workloads)
+       python tests/golden/make_fixtures.py full     (configurations 2 and 3 at full size)
 """
 
 from __future__ import annotations
@@ -28,7 +30,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("BWPM_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("BWPM_REFERENCE", str(REPO.parent / "reference")))
 
 GOLDEN_CASES = (
     "interface_matrices",
@@ -233,7 +235,81 @@ def baseline_shaped_cases() -> None:
     np.savez_compressed(HERE / "workload_cases.npz", **out)
 
 
+FULL_PIXELS = 16384  # pixels of the 3D microlens fields stored in full (a seeded subset)
+FULL_PROJECTIONS = 8  # seeded complex Gaussian projections of each whole 3D field
+
+
+def microlens_probe(n_pixels: int, n_planes: int = 2, seed: int = 31):
+    """Seeded pixel subset (sorted flat indices into (ny·nx)) and projection rows of the 3D
+    microlens check; the GPU test regenerates the same arrays from the same seeds."""
+    rng = np.random.default_rng(seed)
+    pix = np.sort(rng.choice(n_pixels, FULL_PIXELS, replace=False))
+    w = rng.standard_normal((FULL_PROJECTIONS, n_pixels * n_planes)) + 1j * rng.standard_normal(
+        (FULL_PROJECTIONS, n_pixels * n_planes))
+    return pix, w
+
+
+def _full_case(name: str):
+    """One full-size workload through the reference CPU core (run in its own process)."""
+    sys.path.insert(0, str(REPO))
+    from bwpm_b200 import workloads  # noqa: PLC0415
+
+    core = _ref_core()
+    if name.startswith("born2d_"):
+        prob = workloads.born2d(polarization=name.split("_")[1])
+        threads = 1
+    else:
+        prob = workloads.microlens3d()
+        threads = int(os.environ.get("BWPM_FIXTURE_THREADS", "6"))
+    s = core.Solver(*prob.core_args(), threads, fluctuation=prob.fluctuation)
+    res = s.run(prob.field, prob.iterations, [])
+    return name, res["transmitted"], res["reflected"], res["transmitted_iter"], res["reflected_iter"]
+
+
+def full_size_cases() -> None:
+    """Configurations 2 and 3 at full size through the reference CPU core, FP64:
+    - born2d_te / born2d_tm: 4096 points, 2000 slabs with δn on every slab, 6 iterations
+      (inputs from bwpm_b200.workloads.born2d, seed 2): full transmitted and reflected fields
+      and the norms of the per-iteration fields;
+    - microlens3d: 512² points, 400 slabs, 6 iterations (bwpm_b200.workloads.microlens3d, no
+      random input): the fields at a seeded subset of FULL_PIXELS pixels plus FULL_PROJECTIONS
+      seeded complex projections of each whole field (a 512² × 2 complex128 field is 8 MB).
+    The three solves run in parallel processes (a few minutes on 8 cores)."""
+    import multiprocessing as mp  # noqa: PLC0415
+
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(3) as pool:
+        results = pool.map(_full_case, ["born2d_te", "born2d_tm", "microlens3d"])
+    out: dict[str, np.ndarray] = {}
+    for name, t, r, t_it, r_it in results:
+        if name.startswith("born2d_"):
+            out[f"{name}.transmitted"] = t
+            out[f"{name}.reflected"] = r
+            out[f"{name}.transmitted_iter_norms"] = np.array(
+                [np.linalg.norm(x) for x in t_it])
+            out[f"{name}.reflected_iter_norms"] = np.array(
+                [np.linalg.norm(x) for x in r_it])
+        else:
+            n_pix = t.shape[0] * t.shape[1]
+            pix, w = microlens_probe(n_pix)
+            for key, f in (("transmitted", t), ("reflected", r)):
+                flat = f.reshape(n_pix, 2)
+                out[f"{name}.{key}.pixels"] = flat[pix]
+                out[f"{name}.{key}.projections"] = w @ flat.reshape(-1)
+                out[f"{name}.{key}.norm"] = np.array(np.linalg.norm(f))
+                out[f"{name}.{key}.max_abs"] = np.array(np.max(np.abs(f)))
+        print("full-size", name, flush=True)
+    out["meta"] = np.array(json.dumps({
+        "source": "reference CPU core bwpm._core.Solver (cpp/src/solver.cpp:444-528) built by "
+                  "oracle/build_ref.sh; inputs from bwpm_b200.workloads (born2d TE/TM, microlens3d)",
+        "pixels": FULL_PIXELS, "projections": FULL_PROJECTIONS, "probe_seed": 31}))
+    np.savez_compressed(HERE / "full_configs.npz", **out)
+
+
 if __name__ == "__main__":
-    convert_golden()
-    random_volume_cases()
-    baseline_shaped_cases()
+    if sys.argv[1:] == ["full"]:
+        full_size_cases()
+    else:
+        convert_golden()
+        random_volume_cases()
+        baseline_shaped_cases()

@@ -14,7 +14,7 @@ ROOT = Path(__file__).resolve().parents[1]
 def test_reference_arm_prints_one_contract_line():
     out = subprocess.run(
         [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
-         "--warmup", "0", "--cpu-budget", "0.2"],
+         "--warmup", "0", "--reduced", "4,60,1,256", "--ref-sample", "2"],
         cwd=ROOT, capture_output=True, text=True, timeout=600, check=True)
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1, out.stdout

@@ -1,0 +1,80 @@
+"""Configurations 2 and 3 at full size against the reference CPU core (on a GPU).
+
+Fixture tests/golden/full_configs.npz (tests/golden/make_fixtures.py `full`): the reference's
+compiled CPU core (cpp/src/solver.cpp:444-528) on
+- born2d TE and TM: 4096 points, 2000 slabs with Gaussian random δn (std 0.01, 0.5 µm) on every
+  slab, 10° plane wave, 6 iterations (bwpm_b200.workloads.born2d, seed 2);
+- microlens3d: 512² points, 400 slabs, spherical-cap lens n = 1.52 with a 5°-tilted silver back
+  face, mask, 6 iterations (bwpm_b200.workloads.microlens3d), stored as the fields at a seeded
+  subset of 16384 pixels plus 8 seeded complex projections of each whole field.
+FP64 at relative L2 ≤ 1e-10; complex64 at ≤ 1e-4. Behind the silver the transmitted field is
+≈ 1e-94 of the incident one, below the complex64 range (its smallest normal is ≈ 1e-38), so the
+complex64 transmitted field of configuration 3 is checked against a floor of 1e-6 of the
+incident field's norm: ‖E − E_ref‖ ≤ 1e-4 · max(‖E_ref‖, 1e-6 ‖E_in‖).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_npz, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL, C64_TOL = 1e-10, 1e-4
+
+
+@pytest.fixture(scope="module")
+def full():
+    return load_npz("full_configs.npz")
+
+
+def _probe(n_pixels: int):
+    import sys
+
+    from conftest import GOLDEN
+
+    sys.path.insert(0, str(GOLDEN))
+    from make_fixtures import microlens_probe
+
+    return microlens_probe(n_pixels)
+
+
+@pytest.mark.parametrize("pol", ["te", "tm"])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_born2d_full_size(full, pol, precision):
+    from bwpm_b200 import _core, workloads
+
+    p = workloads.born2d(polarization=pol)
+    r = _core.CudaSolver(*p.core_args(), 0, fluctuation=p.fluctuation,
+                         precision=precision).run(p.field, p.iterations, [])
+    tol = FP64_TOL if precision == 64 else C64_TOL
+    for key in ("transmitted", "reflected"):
+        ref = full[f"born2d_{pol}.{key}"]
+        assert rel_l2(r[key], ref) < tol, (key, rel_l2(r[key], ref))
+        norms = np.array([np.linalg.norm(x) for x in r[f"{key}_iter"]])
+        ref_norms = full[f"born2d_{pol}.{key}_iter_norms"]
+        assert np.allclose(norms, ref_norms, rtol=tol, atol=0), key
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_microlens3d_full_size(full, precision):
+    from bwpm_b200 import _core, workloads
+
+    p = workloads.microlens3d()
+    r = _core.CudaSolver(*p.core_args(), 0, precision=precision).run(p.field, p.iterations, [])
+    n_pix = p.ny * p.nx
+    pix, w = _probe(n_pix)
+    tol = FP64_TOL if precision == 64 else C64_TOL
+    e_in = float(np.linalg.norm(p.field))
+    for key in ("transmitted", "reflected"):
+        flat = r[key].reshape(n_pix, 2)
+        ref_pix = full[f"microlens3d.{key}.pixels"]
+        ref_proj = full[f"microlens3d.{key}.projections"]
+        ref_norm = float(full[f"microlens3d.{key}.norm"])
+        floor = 1.0 if precision == 64 else max(1.0, 1e-6 * e_in / ref_norm)
+        assert rel_l2(flat[pix], ref_pix) < tol * floor, (key, rel_l2(flat[pix], ref_pix))
+        proj = w @ flat.reshape(-1)
+        assert np.max(np.abs(proj - ref_proj)) < tol * floor * np.max(np.abs(ref_proj)), key
+        assert abs(np.linalg.norm(flat) - ref_norm) < tol * floor * ref_norm, key

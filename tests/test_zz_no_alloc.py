@@ -82,6 +82,68 @@ def test_noalloc_step_matches_solver_on_two_calls(ny):
     _close(out2, first["transmitted"])
 
 
+def test_noalloc_wide_staging_length_matches_oracle():
+    """7776 = 2^5·3^5 needs the kernel's wider FFT staging (more than 512 threads at 16 values
+    per thread); checked against the CPU oracle's first step (oracle/port.py) at the same
+    tolerance, on two calls in a row."""
+    torch = pytest.importorskip("torch")
+    from bwpm_b200._lib import check, lib
+    from oracle import port
+
+    ny = 7776
+    dy, dz, k0, indices, labels, mask, field = _geometry(ny, 4)
+    lab = labels[1:3].copy()
+    lab[1][: ny // 4] = 2  # air/glass, air/silver and glass/silver pairs in one step
+    ref = port.Solver(ny, 1, dy, 1.0, dz, k0, indices, lab[:, :, None], 1.0 + 0j,
+                      mask[:, None]).run(field, 0, [1, 2])
+    for _ in range(2):
+        st, out = _noalloc(torch, lib, ny, dy, dz, k0, indices, lab[0], lab[1], 1.0, mask,
+                           ref["forward"][1])
+        check(st)
+        _close(out, ref["forward"][2])
+
+
+def test_noalloc_bad_label_then_valid_call_and_no_allocation():
+    """A label outside `indices` is found on the device and returns BWPM_EINVAL with the
+    reference's message; the next valid call starts from a cleared status word and is correct;
+    neither call changes the device's free memory."""
+    torch = pytest.importorskip("torch")
+    from bwpm_b200 import _core
+    from bwpm_b200._lib import BWPM_EINVAL, check, last_error, lib
+
+    ny = 512
+    dy, dz, k0, indices, labels, mask, field = _geometry(ny, 8)
+    dev = torch.device("cuda", 0)
+    bad = labels[0].copy()
+    bad[ny // 3] = indices.size  # one label equal to m
+    d_bad = torch.from_numpy(bad).to(dev)
+    d_good = torch.from_numpy(np.ascontiguousarray(labels[0])).to(dev)
+    d_mask = torch.from_numpy(np.ascontiguousarray(mask)).to(dev)
+    fin = torch.from_numpy(np.ascontiguousarray(field.reshape(ny, 2))).to(dev)
+    fout = torch.zeros_like(fin)
+    idx = np.ascontiguousarray(indices, dtype=np.complex128)
+
+    def call(d_lab):
+        return lib.bwpm_step2d_noalloc(0, ny, dy, dz, k0, idx.ctypes.data, idx.size, None,
+                                       d_lab.data_ptr(), 1.0, 0.0, d_mask.data_ptr(),
+                                       fin.data_ptr(), fout.data_ptr(), None)
+
+    check(call(d_good))  # the module and the scratch address are set up before measuring
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    st = call(d_bad)
+    assert st == BWPM_EINVAL
+    assert "labels must index into" in last_error()
+    fout.zero_()
+    torch.cuda.synchronize()
+    check(call(d_good))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    first = _core.CudaSolver(ny, 1, dy, 1.0, dz, k0, indices, labels[:1, :, None], 1.0 + 0j,
+                             mask[:, None], 0).run(field, 0, [])
+    _close(fout.cpu().numpy().reshape(ny, 1, 2), first["transmitted"])
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     torch = pytest.importorskip("torch")
     from bwpm_b200._lib import BWPM_EINVAL, last_error, lib
