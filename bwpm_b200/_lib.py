@@ -68,6 +68,10 @@ SIGNATURES: dict[str, tuple] = {
     "bwpm_server_result": (_i, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, _p, _p, _p]),
     "bwpm_server_stats": (_i, [_p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
     "bwpm_server_destroy": (None, [_p]),
+    "bwpm_port_power": (_i, [_i, _sz, _sz, _d, _d, _d, _d, _d, _i, _p, ctypes.POINTER(_d)]),
+    "bwpm_plane_power": (_i, [_i, _sz, _sz, _d, _d, _d, _d, _p, ctypes.POINTER(_d)]),
+    "bwpm_axial_focus": (_i, [_i, _sz, _sz, _d, _d, _d, _d, _p, _sz, _d, _p, ctypes.POINTER(_d),
+                              ctypes.POINTER(_d), _p]),
     "bwpm_flush_l2": (_i, [_i, _sz]),
     "bwpm_step2d_noalloc": (_i, [_i, _sz, _d, _d, _d, _p, _sz, _p, _p, _d, _d, _p, _p, _p, _p]),
     "bwpm_host_register": (_i, [_p, _sz]),

@@ -6,7 +6,9 @@
 
 #include "../../include/bwpm_b200.h"
 #include "batch2d.hpp"
+#include "devbuf.hpp"
 #include "noalloc.hpp"
+#include "postproc.hpp"
 #include "server.hpp"
 #include "solver.hpp"
 #include "variants.hpp"
@@ -427,6 +429,63 @@ int bwpm_server_stats(bwpm_server* s, int64_t* submitted, int64_t* completed, in
 }
 
 void bwpm_server_destroy(bwpm_server* s) { delete s; }
+
+namespace {
+bwpm::PlaneGeometry plane_geometry(size_t ny, size_t nx, double dy, double dx, double k0) {
+  if (ny < 1 || nx < 1 || ny > (1u << 20) || nx > (1u << 20))
+    throw bwpm::invalid_argument("ny and nx must be in [1, 2^20]");
+  bwpm::PlaneGeometry g;
+  g.ny = static_cast<int>(ny);
+  g.nx = static_cast<int>(nx);
+  g.dy = dy;
+  g.dx = dx;
+  g.k0 = k0;
+  return g;
+}
+
+// a stream of the call's own on `device`
+struct CallStream {
+  bwpm::OwnedStream s;
+  explicit CallStream(int device) {
+    bwpm::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    s.create();
+  }
+};
+}  // namespace
+
+int bwpm_port_power(int device, size_t ny, size_t nx, double dy, double dx, double k0,
+                    double index_re, double index_im, int direction, const double* field,
+                    double* power) {
+  return guarded([&] {
+    if (!field || !power) throw bwpm::invalid_argument("null array");
+    const bwpm::PlaneGeometry g = plane_geometry(ny, nx, dy, dx, k0);
+    CallStream cs(device);
+    *power = bwpm::port_power(g, as_cd(field), false, bwpm::cd{index_re, index_im}, direction,
+                              cs.s);
+  });
+}
+
+int bwpm_plane_power(int device, size_t ny, size_t nx, double dy, double dx, double k0,
+                     double index, const double* field, double* power) {
+  return guarded([&] {
+    if (!field || !power) throw bwpm::invalid_argument("null array");
+    const bwpm::PlaneGeometry g = plane_geometry(ny, nx, dy, dx, k0);
+    CallStream cs(device);
+    *power = bwpm::plane_power(g, as_cd(field), false, index, cs.s);
+  });
+}
+
+int bwpm_axial_focus(int device, size_t ny, size_t nx, double dy, double dx, double k0,
+                     double index, const double* offsets, size_t noffsets, double na,
+                     const double* field, double* best, double* peak, double* intensity) {
+  return guarded([&] {
+    if (!field || !offsets || !best || !peak) throw bwpm::invalid_argument("null array");
+    const bwpm::PlaneGeometry g = plane_geometry(ny, nx, dy, dx, k0);
+    CallStream cs(device);
+    bwpm::axial_focus(g, as_cd(field), false, index, offsets, noffsets, na, best, peak, intensity,
+                      cs.s);
+  });
+}
 
 int bwpm_flush_l2(int device, size_t bytes) {
   return guarded([&] {

@@ -199,6 +199,33 @@ int bwpm_server_stats(bwpm_server* s, int64_t* submitted, int64_t* completed, in
 
 void bwpm_server_destroy(bwpm_server* s);
 
+/* ---- post-processing of fields on the device (FP64, compensated sums) ----------------------
+ * `field`: host complex128 (ny, nx, 2) (E_x, E_y) on the centred grid; k grids of
+ * numpy.fft.fftfreq; the angular spectrum is this library's FP64 FFT.
+ *
+ * Replaces bwpm.adapter.port_power (src/bwpm/adapter.py:267-284): the Poynting flux through a
+ * port, Σ Re k_z (|Ê_x|² + |Ê_y|² + |Ê_z|²)·dx·dy/(nx·ny), Ê_z = −direction·k⊥·Ê⊥/k_z, in a
+ * homogeneous medium of complex index (index_re, index_im); direction ±1. With nx = 1 and
+ * dx = 1 this is bwpm.fpwpm.power_flux (src/bwpm/fpwpm.py:205-216), the flux of the facade's
+ * energy residual (src/bwpm/fast.py:148-155). */
+int bwpm_port_power(int device, size_t ny, size_t nx, double dy, double dx, double k0,
+                    double index_re, double index_im, int direction, const double* field,
+                    double* power);
+
+/* Replaces bwpm.pilot_imc3d.plane_power (src/bwpm/pilot_imc3d.py:55-67): n Σ cos θ (|E_s|² +
+ * |E_p|²) over the propagating modes of a medium of real index n. */
+int bwpm_plane_power(int device, size_t ny, size_t nx, double dy, double dx, double k0,
+                     double index, const double* field, double* power);
+
+/* Replaces bwpm.pilot_imc3d.axial_focus (src/bwpm/pilot_imc3d.py:96-131): the on-axis
+ * intensity at each of `noffsets` distances (mm, along the direction of travel) of the
+ * propagating modes (with na > 0 only those with k⊥ ≤ na·k0); returns the first offset of the
+ * largest intensity (*best) and that intensity (*peak); `intensity` (noffsets doubles, or NULL)
+ * receives every value. */
+int bwpm_axial_focus(int device, size_t ny, size_t nx, double dy, double dx, double k0,
+                     double index, const double* offsets, size_t noffsets, double na,
+                     const double* field, double* best, double* peak, double* intensity);
+
 /* Writes `bytes` of scratch memory on `device` (evicts the 126 MB L2 between timed runs). */
 int bwpm_flush_l2(int device, size_t bytes);
 

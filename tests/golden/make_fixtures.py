@@ -16,6 +16,7 @@ these fixtures:
 
 Usage: python tests/golden/make_fixtures.py          (golden files, random volumes, workloads)
        python tests/golden/make_fixtures.py full     (configurations 2 and 3 at full size)
+       python tests/golden/make_fixtures.py post     (post-processing of fields)
 """
 
 from __future__ import annotations
@@ -306,9 +307,79 @@ def full_size_cases() -> None:
     np.savez_compressed(HERE / "full_configs.npz", **out)
 
 
+def post_cases() -> None:
+    """Post-processing of fields by the reference's own functions on seeded inputs:
+    bwpm.adapter.port_power (src/bwpm/adapter.py:267-284), bwpm.pilot_imc3d.plane_power and
+    axial_focus (src/bwpm/pilot_imc3d.py:55-131), bwpm.fpwpm.power_flux
+    (src/bwpm/fpwpm.py:205-216)."""
+    sys.path.insert(0, str(REF / "src"))
+    from bwpm.adapter import Port, PortField, port_power  # noqa: PLC0415
+    from bwpm.fpwpm import Grid2D, power_flux  # noqa: PLC0415
+    from bwpm.pilot_imc3d import axial_focus, plane_power  # noqa: PLC0415
+    from bwpm.volume3d import Grid3D  # noqa: PLC0415
+
+    rng = np.random.default_rng(41)
+    out: dict[str, np.ndarray] = {}
+    wl = 0.633
+    lam = wl * 1e-3
+    # a tilted Gaussian beam in both components plus seeded noise, 48 x 64
+    ny, nx, d = 48, 64, lam / 6
+    y = (np.arange(ny) - ny // 2) * d
+    x = (np.arange(nx) - nx // 2) * d
+    r2 = y[:, None] ** 2 + x[None, :] ** 2
+    k0 = 2 * np.pi / lam
+    beam = np.exp(-r2 / (8 * d) ** 2) * np.exp(1j * 0.3 * k0 * x[None, :])
+    field = np.stack([beam, 0.4j * beam], axis=-1)
+    field = field + 0.05 * (rng.standard_normal(field.shape) + 1j * rng.standard_normal(field.shape))
+    out["beam3d.field"] = field
+    out["beam3d.grid"] = np.array([ny, nx, d, d, wl])
+    for tag, index, direction in (("n15_fwd", 1.5 + 0j, 1), ("absorbing_bwd", 1.0 + 0.02j, -1),
+                                  ("silver_fwd", 0.135 + 3.98j, 1)):
+        port = Port(0.0, direction, index, wl, nx, ny, d, d)
+        out[f"beam3d.port_power.{tag}"] = np.array(port_power(PortField(port, field)))
+        out[f"beam3d.port_power.{tag}.index"] = np.array(index)
+        out[f"beam3d.port_power.{tag}.direction"] = np.array(direction)
+    grid = Grid3D(nx, ny, d, d, d, wl)
+    out["beam3d.plane_power.n15"] = np.array(plane_power(field, grid, 1.5))
+    out["beam3d.plane_power.n10"] = np.array(plane_power(field, grid, 1.0))
+    # a converging Gaussian beam (focus 30 µm behind the plane), 64 x 64, in air
+    n, d = 64, lam / 4
+    c = (np.arange(n) - n // 2) * d
+    r2 = c[:, None] ** 2 + c[None, :] ** 2
+    f = 30e-3
+    beam = np.exp(-r2 / (14 * d) ** 2) * np.exp(-1j * k0 * r2 / (2 * f))
+    lens = np.stack([beam, 0.2 * beam], axis=-1)
+    offsets = np.linspace(0.0, 60e-3, 61)
+    out["focus.field"] = lens
+    out["focus.grid"] = np.array([n, n, d, d, wl])
+    out["focus.offsets"] = offsets
+    g = Grid3D(n, n, d, d, d, wl)
+    for tag, na in (("all", None), ("na04", 0.4)):
+        best, peak = axial_focus(lens, g, 1.0, offsets, na=na)
+        out[f"focus.{tag}.best"] = np.array(best)
+        out[f"focus.{tag}.peak"] = np.array(peak)
+    # 2D power flux (nx = 1), 256 points
+    ny, d = 256, lam / 8
+    y = (np.arange(ny) - ny // 2) * d
+    prof = np.exp(-(y / (20 * d)) ** 2) * np.exp(1j * 0.2 * k0 * y)
+    f2 = np.stack([prof, 0.5 * prof], axis=-1) + 0.02 * rng.standard_normal((ny, 2))
+    g2 = Grid2D(ny, d, d, wl)
+    out["flux2d.field"] = f2
+    out["flux2d.grid"] = np.array([ny, 1, d, 1.0, wl])
+    out["flux2d.power_flux.n15_fwd"] = np.array(power_flux(f2, g2, 1.5 + 0j, direction=1))
+    out["flux2d.power_flux.n10_bwd"] = np.array(power_flux(f2, g2, 1.0 + 0j, direction=-1))
+    out["meta"] = np.array(json.dumps({"source": "reference functions (adapter.port_power, "
+                                                 "pilot_imc3d.plane_power/axial_focus, "
+                                                 "fpwpm.power_flux) on seeded inputs, seed 41"}))
+    np.savez_compressed(HERE / "postproc.npz", **out)
+    print("postproc", sorted(out))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["full"]:
         full_size_cases()
+    elif sys.argv[1:] == ["post"]:
+        post_cases()
     else:
         convert_golden()
         random_volume_cases()
