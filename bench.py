@@ -352,12 +352,21 @@ def run_ours(args) -> None:
     rng = np.random.default_rng(7)
     sample = [int(i) for i in rng.permutation(count)[: args.fp64_sample]]
     fp64_t, errs, eps_err = [], [], []
+    ref_cuda = _reference_cuda_core()
+    ref_t, ref_diff = [], []
     for i in sample:
         p = workloads.tilted_slab2d_from(params[i])
         s = _core.CudaSolver(*p.core_args(), device)
         t0 = time.perf_counter()
         r64 = s.run(p.field, p.iterations, [])
         fp64_t.append(time.perf_counter() - t0)
+        if ref_cuda is not None:  # the reference's own GPU core (cuFFT, FP64) on the same solve
+            rs = ref_cuda.CudaSolver(*p.core_args(), device)
+            t0 = time.perf_counter()
+            rr = rs.run(p.field, p.iterations, [])
+            ref_t.append(time.perf_counter() - t0)
+            ref_diff.append(max(_rel(r64[k], rr[k]) for k in ("transmitted", "reflected")))
+            del rs, rr
         r32 = b.result(i)
         for key in ("transmitted", "reflected"):
             ref = r64[key][:, 0]
@@ -375,6 +384,7 @@ def run_ours(args) -> None:
     mean_cost = np.mean([prm["ny"] * np.log2(prm["ny"]) * prm["nz"] for prm in params])
     samp_cost = np.mean([params[i]["ny"] * np.log2(params[i]["ny"]) * params[i]["nz"] for i in sample]) if sample else 1.0
     fp64_rate = 1.0 / (np.mean(fp64_t) * mean_cost / samp_cost) if sample else None
+    ref_cuda_rate = 1.0 / (np.mean(ref_t) * mean_cost / samp_cost) if ref_t else None
     # roofline of the resident kernel: algorithmic FLOPs per launch ÷ launch time
     kern_s = step_ms * 1e-3
     achieved = work["flops"] / kern_s / 1e12
@@ -405,7 +415,14 @@ def run_ours(args) -> None:
         "fp64_plain": {"value": fp64_rate, "unit": "solves/s", "sample": len(sample),
                        "note": "per-solve FP64 CudaSolver (drop-in path), mean sample time scaled "
                                "to the batch's mean N·log2N·nz",
-                       "speedup_batched_c64": value / ws / fp64_rate if fp64_rate else None},
+                       "speedup_batched_c64": value / ws / fp64_rate if fp64_rate else None,
+                       "reference_cuda_core": {
+                           "value": ref_cuda_rate, "unit": "solves/s",
+                           "note": "the reference's own CudaSolver (cuFFT, FP64; built for "
+                                   "sm_100a from its sources) on the same sample and scaling",
+                           "rel_l2_vs_ours_fp64_max": max(ref_diff) if ref_diff else None,
+                           "speedup_batched_c64": value / ws / ref_cuda_rate
+                           if ref_cuda_rate else None}},
         "l2_err_max": float(np.max(errs)) if errs else None,
         "eps_err_max": float(np.max(eps_err)) if eps_err else None,
         "eps_err_note": "|eps_c64 - eps_fp64| / max(1, (P_R + P_T)/P_in) over the sample's iterations",
@@ -513,6 +530,39 @@ def run_served(device: int, fp64_sample: int) -> dict:
 
 # ---- the other configurations (parity and timing beside the headline; not part of its value) ----
 
+_REF_CORE: dict = {}
+
+
+def _reference_core():
+    """The reference's compiled bwpm._core, loaded once per process: the staged install in
+    baseline/_ref (oracle/stage_reference.sh; CPU Solver and its own CUDA core) where present,
+    else the CPU core of oracle/_ref; None when neither exists. (Both register the same C++
+    types with pybind11, so only one of them can be loaded in a process.)"""
+    if "core" not in _REF_CORE:
+        import importlib.util
+
+        mod = None
+        for d in (ROOT / "baseline" / "_ref" / "bwpm", ROOT / "oracle" / "_ref"):
+            so = sorted(d.glob("_core*.so"))
+            if not so:
+                continue
+            try:
+                spec = importlib.util.spec_from_file_location("_core", so[0])
+                mod = importlib.util.module_from_spec(spec)
+                spec.loader.exec_module(mod)
+                break
+            except ImportError:
+                mod = None
+        _REF_CORE["core"] = mod
+    return _REF_CORE["core"]
+
+
+def _reference_cuda_core():
+    """The reference core when it has its CUDA backend (the staged install), else None."""
+    mod = _reference_core()
+    return mod if mod is not None and getattr(mod, "HAS_CUDA", False) else None
+
+
 def run_configs(device: int) -> dict:
     """Configurations 1-3 on this GPU: complex64 result of this implementation against the
     per-solve FP64 drop-in path (time and relative L2 error), and for the 2D slab the reference's
@@ -533,14 +583,7 @@ def run_configs(device: int) -> dict:
     b.prepare()
     b.run()
     batch_ms = b.run()
-    ref_core = None
-    so = sorted((ROOT / "oracle" / "_ref").glob("_core*.so"))
-    if so:
-        import importlib.util
-
-        spec = importlib.util.spec_from_file_location("_core", so[0])  # its init symbol
-        ref_core = importlib.util.module_from_spec(spec)
-        spec.loader.exec_module(ref_core)
+    ref_core = _reference_core()
     t64, tcpu, errs = [], [], []
     for p, i in zip(probs, ids):
         r64, dt = timed(lambda p=p: _core.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))

@@ -9,6 +9,7 @@
 // - selection, mask, reflection gather and sparse source add are fused into the inverse
 //   transform's epilogue; interface pixel lists and source stores are allocated once.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <set>
@@ -20,6 +21,7 @@
 #include "devbuf.hpp"
 #include "plan.hpp"
 #include "plane_kernels.cuh"
+#include "plane_setup.cuh"
 #include "solver.hpp"
 
 namespace bwpm {
@@ -56,6 +58,8 @@ class PlaneSolver final : public Solver {
  private:
   using C = cx<T>;
   void setup();
+  // per-step pairs, pair-id planes and interface lists from uint8 labels on the device
+  void device_steps(const std::uint8_t* labels_u8);
   const C* table(int kind, cd nr, cd ns);
   StepPasses passes(int step, bool backward, bool reflect);
   // x_ready: xbuf_ already holds the x transform of `in` (3D, fused into the previous step);
@@ -157,10 +161,15 @@ void PlaneSolver<T>::setup() {
   const std::size_t nn = n();
   if (in_.ny < 1 || in_.nx < 1) throw invalid_argument("ny and nx must be positive");
   const std::int32_t* labels = in_.labels_view ? in_.labels_view : in_.labels.data();
-  if (!in_.labels_view && in_.labels.size() != in_.nz * nn)
+  if (in_.labels_device) {  // uint8 labels on the device (generated there; in range by construction)
+    if (in_.indices.size() > 255) throw invalid_argument("device labels take at most 255 materials");
+    if (!in_.fluct.empty()) throw invalid_argument("fluctuation needs host labels");
+    labels = nullptr;
+  } else if (!in_.labels_view && in_.labels.size() != in_.nz * nn) {
     throw invalid_argument("labels must have shape (nz, ny, nx)");
+  }
   if (!in_.mask.empty() && in_.mask.size() != nn) throw invalid_argument("mask must have shape (ny, nx)");
-  {  // range check as a min/max reduction (vectorises; one pass over the labels)
+  if (labels) {  // range check as a min/max reduction (vectorises; one pass over the labels)
     std::int32_t lo = 0, hi = 0;
     const std::size_t nl = in_.nz * nn;
     if (nl > 0) lo = hi = labels[0];
@@ -210,103 +219,145 @@ void PlaneSolver<T>::setup() {
   upload_tw(hy_, tw_y_);
   upload_tw(hx_, tw_x_);
 
-  // per-step pairs, pair-id planes (deduplicated), interface lists
-  std::vector<std::uint8_t> pid_host;
-  std::unordered_map<std::uint64_t, std::vector<long long>> pid_seen;
-  std::vector<int> iface_host, rowoff_host;
-  std::vector<std::int32_t> before(nn, -1);
-  steps_.resize(in_.nz);
-  std::vector<std::uint8_t> pid(nn);
-  // a label pair (r, s), r ∈ [−1, m), s ∈ [0, m), as one code (r + 1)·m + s: codes sort like the
-  // pairs, so a presence scan lists a step's pairs in the reference's std::set order
-  // (cpp/src/solver.cpp:389-390); per code: whether the indices differ (an interface)
-  const int m = static_cast<int>(in_.indices.size());
-  const std::size_t ncode = static_cast<std::size_t>(m + 1) * m;
-  std::vector<std::uint8_t> code_iface(ncode);
-  for (int r = -1; r < m; ++r)
-    for (int q = 0; q < m; ++q) {
-      const cd x = index_of(r), y = index_of(q);
-      code_iface[static_cast<std::size_t>(r + 1) * m + q] = x.re != y.re || x.im != y.im;
-    }
-  std::vector<std::uint32_t> code(nn), stamp(ncode, 0);
-  std::vector<int> code_id(ncode, -1);
-  for (std::size_t p = 0; p < in_.nz; ++p) {
-    const std::int32_t* a = p == 0 ? before.data() : labels + (p - 1) * nn;
-    const std::int32_t* b = labels + p * nn;
-    const std::uint32_t mark = static_cast<std::uint32_t>(p) + 1;
-    std::vector<std::uint32_t> present;
-    for (std::size_t q = 0; q < nn; ++q) {
-      const std::uint32_t k = static_cast<std::uint32_t>(a[q] + 1) * m + b[q];
-      code[q] = k;
-      if (stamp[k] != mark) {
-        stamp[k] = mark;
-        present.push_back(k);
+  // per-step pairs, pair-id planes and interface lists: on the device for large volumes (or
+  // labels already on the device), else on the host (pair-id planes deduplicated); the
+  // environment variable BWPM_SETUP=host|device overrides the choice where both can run
+  bool on_device = in_.labels_device != nullptr ||
+                   (in_.indices.size() <= 255 && in_.nz * nn >= (std::size_t{1} << 22));
+  if (const char* e = std::getenv("BWPM_SETUP"); e && !in_.labels_device) {
+    if (std::strcmp(e, "host") == 0) on_device = false;
+    if (std::strcmp(e, "device") == 0) on_device = in_.indices.size() <= 255;
+  }
+  if (in_.nz > 65535) {
+    if (in_.labels_device) throw invalid_argument("device labels take at most 65535 slabs");
+    on_device = false;
+  }
+  if (on_device) {
+    DevBuf<std::uint8_t> u8;
+    const std::uint8_t* lab8 = in_.labels_device;
+    if (!lab8) {  // upload the caller's int32 labels in chunks of planes, as uint8
+      u8.alloc(std::max<std::size_t>(1, in_.nz * nn), stream_);
+      const std::size_t per = std::max<std::size_t>(1, (std::size_t{64} << 20) / (4 * nn));
+      DevBuf<std::int32_t> stage(std::min(per, in_.nz) * nn, stream_);
+      DevBuf<int> bad(1, stream_);
+      check_cuda(cudaMemsetAsync(bad.ptr, 0, sizeof(int), stream_), "memset");
+      for (std::size_t p0 = 0; p0 < in_.nz; p0 += per) {
+        const std::size_t cnt = std::min(per, in_.nz - p0) * nn;
+        check_cuda(cudaMemcpyAsync(stage.ptr, labels + p0 * nn, cnt * sizeof(std::int32_t),
+                                   cudaMemcpyHostToDevice, stream_), "labels upload");
+        k_labels_to_u8<<<std::min<long long>(ceil_div(static_cast<long long>(cnt), 256), 4 * sms_), 256, 0,
+                         stream_>>>(stage.ptr, u8.ptr + p0 * nn, static_cast<long long>(cnt), static_cast<int>(in_.indices.size()),
+                                    bad.ptr);
+        check_cuda(cudaGetLastError(), "k_labels_to_u8");
       }
+      lab8 = u8.ptr;
+      device_steps(lab8);
+      int flag = 0;
+      check_cuda(cudaMemcpy(&flag, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost), "labels check");
+      if (flag) throw invalid_argument("labels must index into `indices`");
+    } else {
+      device_steps(lab8);
     }
-    std::sort(present.begin(), present.end());
-    StepInfo& st = steps_[p];
-    st.pairs.clear();
-    for (auto k : present) st.pairs.emplace_back(static_cast<int>(k / m) - 1, static_cast<int>(k % m));
-    if (st.pairs.size() > 255) throw invalid_argument("more than 255 label pairs in one step");
-    if (2 * st.pairs.size() > static_cast<std::size_t>(kMaxPasses))
-      throw invalid_argument("too many label pairs in one step");
-    if (st.pairs.size() > 1) {
-      for (std::size_t i = 0; i < present.size(); ++i) code_id[present[i]] = static_cast<int>(i);
-      std::uint64_t h = 1469598103934665603ULL;
+    in_.labels_device = nullptr;  // not read after set-up
+  } else {
+    // per-step pairs, pair-id planes (deduplicated), interface lists
+    std::vector<std::uint8_t> pid_host;
+    std::unordered_map<std::uint64_t, std::vector<long long>> pid_seen;
+    std::vector<int> iface_host, rowoff_host;
+    std::vector<std::int32_t> before(nn, -1);
+    steps_.resize(in_.nz);
+    std::vector<std::uint8_t> pid(nn);
+    // a label pair (r, s), r ∈ [−1, m), s ∈ [0, m), as one code (r + 1)·m + s: codes sort like the
+    // pairs, so a presence scan lists a step's pairs in the reference's std::set order
+    // (cpp/src/solver.cpp:389-390); per code: whether the indices differ (an interface)
+    const int m = static_cast<int>(in_.indices.size());
+    const std::size_t ncode = static_cast<std::size_t>(m + 1) * m;
+    std::vector<std::uint8_t> code_iface(ncode);
+    for (int r = -1; r < m; ++r)
+      for (int q = 0; q < m; ++q) {
+        const cd x = index_of(r), y = index_of(q);
+        code_iface[static_cast<std::size_t>(r + 1) * m + q] = x.re != y.re || x.im != y.im;
+      }
+    std::vector<std::uint32_t> code(nn), stamp(ncode, 0);
+    std::vector<int> code_id(ncode, -1);
+    for (std::size_t p = 0; p < in_.nz; ++p) {
+      const std::int32_t* a = p == 0 ? before.data() : labels + (p - 1) * nn;
+      const std::int32_t* b = labels + p * nn;
+      const std::uint32_t mark = static_cast<std::uint32_t>(p) + 1;
+      std::vector<std::uint32_t> present;
       for (std::size_t q = 0; q < nn; ++q) {
-        pid[q] = static_cast<std::uint8_t>(code_id[code[q]]);
-        h = (h ^ pid[q]) * 1099511628211ULL;
-      }
-      long long found = -1;
-      for (long long off : pid_seen[h])
-        if (std::memcmp(pid_host.data() + off, pid.data(), nn) == 0) {
-          found = off;
-          break;
+        const std::uint32_t k = static_cast<std::uint32_t>(a[q] + 1) * m + b[q];
+        code[q] = k;
+        if (stamp[k] != mark) {
+          stamp[k] = mark;
+          present.push_back(k);
         }
-      if (found < 0) {
-        found = static_cast<long long>(pid_host.size());
-        pid_host.insert(pid_host.end(), pid.begin(), pid.end());
-        pid_seen[h].push_back(found);
       }
-      st.pid_off = found;
+      std::sort(present.begin(), present.end());
+      StepInfo& st = steps_[p];
+      st.pairs.clear();
+      for (auto k : present) st.pairs.emplace_back(static_cast<int>(k / m) - 1, static_cast<int>(k % m));
+      if (st.pairs.size() > 255) throw invalid_argument("more than 255 label pairs in one step");
+      if (2 * st.pairs.size() > static_cast<std::size_t>(kMaxPasses))
+        throw invalid_argument("too many label pairs in one step");
+      if (st.pairs.size() > 1) {
+        for (std::size_t i = 0; i < present.size(); ++i) code_id[present[i]] = static_cast<int>(i);
+        std::uint64_t h = 1469598103934665603ULL;
+        for (std::size_t q = 0; q < nn; ++q) {
+          pid[q] = static_cast<std::uint8_t>(code_id[code[q]]);
+          h = (h ^ pid[q]) * 1099511628211ULL;
+        }
+        long long found = -1;
+        for (long long off : pid_seen[h])
+          if (std::memcmp(pid_host.data() + off, pid.data(), nn) == 0) {
+            found = off;
+            break;
+          }
+        if (found < 0) {
+          found = static_cast<long long>(pid_host.size());
+          pid_host.insert(pid_host.end(), pid.begin(), pid.end());
+          pid_seen[h].push_back(found);
+        }
+        st.pid_off = found;
+      }
+      st.iface_off = static_cast<long long>(iface_host.size());
+      bool any_iface = false;
+      for (auto k : present) any_iface |= code_iface[k] != 0;
+      if (any_iface)
+        for (std::size_t q = 0; q < nn; ++q)
+          if (code_iface[code[q]]) iface_host.push_back(static_cast<int>(q));
+      st.niface = static_cast<int>(iface_host.size() - st.iface_off);
+      if (st.niface > 0 && !is2d()) {
+        st.rowoff_off = static_cast<long long>(rowoff_host.size());
+        const int* first = iface_host.data() + st.iface_off;
+        for (std::size_t y = 0; y <= in_.ny; ++y)
+          rowoff_host.push_back(static_cast<int>(
+              std::lower_bound(first, first + st.niface, static_cast<int>(y * in_.nx)) - first));
+      }
+      st.host_slot = host_of[p];
+      int npass = static_cast<int>(st.pairs.size());
+      for (auto& pr : st.pairs) {
+        const cd x = index_of(pr.first), y = index_of(pr.second);
+        if (x.re != y.re || x.im != y.im) ++npass;
+      }
+      max_pass_ = std::max(max_pass_, npass);
     }
-    st.iface_off = static_cast<long long>(iface_host.size());
-    bool any_iface = false;
-    for (auto k : present) any_iface |= code_iface[k] != 0;
-    if (any_iface)
-      for (std::size_t q = 0; q < nn; ++q)
-        if (code_iface[code[q]]) iface_host.push_back(static_cast<int>(q));
-    st.niface = static_cast<int>(iface_host.size() - st.iface_off);
-    if (st.niface > 0 && !is2d()) {
-      st.rowoff_off = static_cast<long long>(rowoff_host.size());
-      const int* first = iface_host.data() + st.iface_off;
-      for (std::size_t y = 0; y <= in_.ny; ++y)
-        rowoff_host.push_back(static_cast<int>(
-            std::lower_bound(first, first + st.niface, static_cast<int>(y * in_.nx)) - first));
+    in_.labels_view = nullptr;  // the caller's labels are not read after set-up
+    iface_total_ = static_cast<long long>(iface_host.size());
+    if (!pid_host.empty()) {
+      pid_pool_.alloc(pid_host.size(), stream_);
+      pid_pool_.upload(pid_host.data(), pid_host.size());
     }
-    st.host_slot = host_of[p];
-    int npass = static_cast<int>(st.pairs.size());
-    for (auto& pr : st.pairs) {
-      const cd x = index_of(pr.first), y = index_of(pr.second);
-      if (x.re != y.re || x.im != y.im) ++npass;
+    if (!iface_host.empty()) {
+      iface_pool_.alloc(iface_host.size(), stream_);
+      iface_pool_.upload(iface_host.data(), iface_host.size());
+      src_fwd_.alloc(2 * iface_host.size(), stream_);
+      src_bwd_.alloc(2 * iface_host.size(), stream_);
     }
-    max_pass_ = std::max(max_pass_, npass);
-  }
-  in_.labels_view = nullptr;  // the caller's labels are not read after set-up
-  iface_total_ = static_cast<long long>(iface_host.size());
-  if (!pid_host.empty()) {
-    pid_pool_.alloc(pid_host.size(), stream_);
-    pid_pool_.upload(pid_host.data(), pid_host.size());
-  }
-  if (!iface_host.empty()) {
-    iface_pool_.alloc(iface_host.size(), stream_);
-    iface_pool_.upload(iface_host.data(), iface_host.size());
-    src_fwd_.alloc(2 * iface_host.size(), stream_);
-    src_bwd_.alloc(2 * iface_host.size(), stream_);
-  }
-  if (!rowoff_host.empty()) {
-    rowoff_pool_.alloc(rowoff_host.size(), stream_);
-    rowoff_pool_.upload(rowoff_host.data(), rowoff_host.size());
+    if (!rowoff_host.empty()) {
+      rowoff_pool_.alloc(rowoff_host.size(), stream_);
+      rowoff_pool_.upload(rowoff_host.data(), rowoff_host.size());
+    }
   }
   if (!in_.mask.empty()) {  // FP32: hi values then lo values (mask = hi + lo)
     const bool pair = sizeof(T) != sizeof(double);
@@ -370,6 +421,116 @@ void PlaneSolver<T>::setup() {
     partial_host_.resize(1024);
   }
   check_cuda(cudaStreamSynchronize(stream_), "setup");  // this solver's stream only
+}
+
+template <typename T>
+void PlaneSolver<T>::device_steps(const std::uint8_t* labels_u8) {
+  const std::size_t nn = n();
+  const int nz = static_cast<int>(in_.nz);
+  const int m = static_cast<int>(in_.indices.size());
+  const int ncode = (m + 1) * m;
+  const int words = (ncode + 31) / 32;
+  std::vector<std::uint8_t> code_iface(ncode);
+  for (int r = -1; r < m; ++r)
+    for (int q = 0; q < m; ++q) {
+      const cd x = index_of(r), y = index_of(q);
+      code_iface[static_cast<std::size_t>(r + 1) * m + q] = x.re != y.re || x.im != y.im;
+    }
+  SetupVolume v{labels_u8, static_cast<long long>(nn), nz, static_cast<int>(in_.ny),
+                static_cast<int>(in_.nx), m, words};
+  DevBuf<std::uint8_t> d_iface(ncode, stream_);
+  d_iface.upload(code_iface.data(), code_iface.size());
+  DevBuf<unsigned> bits(static_cast<std::size_t>(nz) * words, stream_);
+  DevBuf<unsigned long long> counts(nz, stream_);
+  check_cuda(cudaMemsetAsync(bits.ptr, 0, bits.bytes(), stream_), "memset");
+  check_cuda(cudaMemsetAsync(counts.ptr, 0, counts.bytes(), stream_), "memset");
+  const int per_step = static_cast<int>(std::max<long long>(
+      1, std::min<long long>(ceil_div(static_cast<long long>(nn), 256LL * 8), 64)));
+  k_setup_presence<<<dim3(per_step, nz), 256, words * sizeof(unsigned), stream_>>>(v, d_iface.ptr,
+                                                                                 bits.ptr, counts.ptr);
+  check_cuda(cudaGetLastError(), "k_setup_presence");
+  std::vector<unsigned> h_bits(bits.n);
+  std::vector<unsigned long long> h_counts(nz);
+  check_cuda(cudaMemcpyAsync(h_bits.data(), bits.ptr, bits.bytes(), cudaMemcpyDeviceToHost, stream_), "bits");
+  check_cuda(cudaMemcpyAsync(h_counts.data(), counts.ptr, counts.bytes(), cudaMemcpyDeviceToHost, stream_),
+             "counts");
+  check_cuda(cudaStreamSynchronize(stream_), "setup presence");
+  // pairs per step in code order (the reference's std::set order), offsets of the pools
+  std::vector<int> multi, with_iface;
+  std::vector<long long> pid_off, iface_off, rowoff_off;
+  std::vector<std::uint8_t> code_id;
+  long long pid_total = 0, iface_total = 0, rowoff_total = 0;
+  steps_.assign(in_.nz, StepInfo{});
+  for (int p = 0; p < nz; ++p) {
+    StepInfo& st = steps_[p];
+    const unsigned* b = h_bits.data() + static_cast<std::size_t>(p) * words;
+    std::vector<int> present;
+    for (int c = 0; c < ncode; ++c)
+      if (b[c >> 5] & (1u << (c & 31))) present.push_back(c);
+    for (int c : present) st.pairs.emplace_back(c / m - 1, c % m);
+    if (st.pairs.size() > 255) throw invalid_argument("more than 255 label pairs in one step");
+    if (2 * st.pairs.size() > static_cast<std::size_t>(kMaxPasses))
+      throw invalid_argument("too many label pairs in one step");
+    if (st.pairs.size() > 1) {
+      st.pid_off = pid_total;
+      multi.push_back(p);
+      pid_off.push_back(pid_total);
+      pid_total += static_cast<long long>(nn);
+      const std::size_t row = code_id.size();
+      code_id.resize(row + ncode, 0);
+      for (std::size_t i = 0; i < present.size(); ++i) code_id[row + present[i]] = static_cast<std::uint8_t>(i);
+    }
+    st.iface_off = iface_total;
+    st.niface = static_cast<int>(h_counts[p]);
+    if (st.niface > 0) {
+      with_iface.push_back(p);
+      iface_off.push_back(iface_total);
+      iface_total += st.niface;
+      if (!is2d()) {
+        st.rowoff_off = rowoff_total;
+        rowoff_off.push_back(rowoff_total);
+        rowoff_total += static_cast<long long>(in_.ny) + 1;
+      } else {
+        rowoff_off.push_back(-1);
+      }
+    }
+    int npass = static_cast<int>(st.pairs.size());
+    for (auto& pr : st.pairs) {
+      const cd x = index_of(pr.first), y = index_of(pr.second);
+      if (x.re != y.re || x.im != y.im) ++npass;
+    }
+    max_pass_ = std::max(max_pass_, npass);
+  }
+  iface_total_ = iface_total;
+  if (!multi.empty()) {
+    pid_pool_.alloc(static_cast<std::size_t>(pid_total), stream_);
+    DevBuf<int> d_steps(multi.size(), stream_);
+    DevBuf<long long> d_off(pid_off.size(), stream_);
+    DevBuf<std::uint8_t> d_code(code_id.size(), stream_);
+    d_steps.upload(multi.data(), multi.size());
+    d_off.upload(pid_off.data(), pid_off.size());
+    d_code.upload(code_id.data(), code_id.size());
+    k_setup_pid<<<dim3(static_cast<unsigned>(std::min<long long>(ceil_div(static_cast<long long>(nn), 256), 64)),
+                       static_cast<unsigned>(multi.size())), 256, 0, stream_>>>(
+        v, d_steps.ptr, d_off.ptr, d_code.ptr, ncode, pid_pool_.ptr);
+    check_cuda(cudaGetLastError(), "k_setup_pid");
+    check_cuda(cudaStreamSynchronize(stream_), "setup pid");
+  }
+  if (!with_iface.empty()) {
+    iface_pool_.alloc(static_cast<std::size_t>(iface_total), stream_);
+    src_fwd_.alloc(2 * static_cast<std::size_t>(iface_total), stream_);
+    src_bwd_.alloc(2 * static_cast<std::size_t>(iface_total), stream_);
+    if (rowoff_total > 0) rowoff_pool_.alloc(static_cast<std::size_t>(rowoff_total), stream_);
+    DevBuf<int> d_steps(with_iface.size(), stream_);
+    DevBuf<long long> d_ioff(iface_off.size(), stream_), d_roff(rowoff_off.size(), stream_);
+    d_steps.upload(with_iface.data(), with_iface.size());
+    d_ioff.upload(iface_off.data(), iface_off.size());
+    d_roff.upload(rowoff_off.data(), rowoff_off.size());
+    k_setup_iface<<<static_cast<unsigned>(with_iface.size()), kSetupThreads, 0, stream_>>>(
+        v, d_steps.ptr, d_ioff.ptr, d_roff.ptr, d_iface.ptr, iface_pool_.ptr, rowoff_pool_.ptr);
+    check_cuda(cudaGetLastError(), "k_setup_iface");
+    check_cuda(cudaStreamSynchronize(stream_), "setup iface");
+  }
 }
 
 template <typename T>

@@ -20,6 +20,9 @@ struct SolverInput {
   // or, when set, the caller's labels read in place during set-up (nz·ny·nx values, valid until
   // the solver has been constructed; `labels` is then empty)
   const std::int32_t* labels_view = nullptr;
+  // or, when set, uint8 labels in device memory (nz·ny·nx values on `device`, e.g. generated
+  // there from a geometry), read during set-up only; at most 255 materials, no fluctuation
+  const std::uint8_t* labels_device = nullptr;
   std::size_t nz = 0;
   cd index_before{1.0, 0.0};
   std::vector<double> mask;          // (ny, nx) or empty

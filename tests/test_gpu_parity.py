@@ -196,3 +196,23 @@ def test_run_twice_is_deterministic(core):
     r2 = s.run(f, 2, [])
     assert np.array_equal(r1["transmitted"], r2["transmitted"])
     assert np.array_equal(r1["reflected"], r2["reflected"])
+
+
+@pytest.mark.parametrize("prefix,iters", [("volume1.", 2), ("volume2.", 2), ("volume3.", 2)])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_device_setup_equals_host_setup(core, monkeypatch, prefix, iters, precision):
+    """The per-step tables built on the device (plane_setup.cuh) give bit-identical results to
+    the host set-up, FP64 and complex64, with keep planes and stored sources."""
+    d = load_npz("random_volumes.npz")
+    args, field, _ = volume_case(d, prefix)
+    out = {}
+    for where in ("host", "device"):
+        monkeypatch.setenv("BWPM_SETUP", where)
+        out[where] = core.CudaSolver(*args, 0, precision=precision).run(field, iters, [0, 5])
+    a, b = out["host"], out["device"]
+    for key in ("transmitted", "reflected"):
+        assert np.array_equal(a[key], b[key]), key
+    for q in (0, 5):
+        assert np.array_equal(a["forward"][q], b["forward"][q])
+        assert np.array_equal(a["backward"][q], b["backward"][q])
+    assert a["stored_values"] == b["stored_values"]
