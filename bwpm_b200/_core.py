@@ -10,7 +10,9 @@ All computation runs on the GPU through libbwpm_b200.so. The reference's CPU cla
 not provided: this package has no CPU path.
 
 Extensions beyond the reference: keyword `precision` (64: complex128 fields, the reference's
-arithmetic; 32: complex64 fields with FP64-built operator tables) and `gmres_tol`.
+arithmetic; 32: complex64 fields with FP64-built operator tables) and `gmres_tol`;
+`CudaSolver.from_geometry` (labels generated on the device from a geometry, see
+bwpm_b200.geometry).
 """
 
 from __future__ import annotations
@@ -89,6 +91,29 @@ class CudaSolver:
                                      ib.imag, ptr(mask_a), int(device), ptr(fl), self.precision,
                                      float(gmres_tol), ctypes.byref(h)))
         self._h = h
+
+    @classmethod
+    def from_geometry(cls, ny, nx, dy, dx, dz, k0, indices, geometry: dict, index_before, mask,
+                      device: int = 0, *, precision: int = 64) -> CudaSolver:
+        """A solver whose labels are generated on the device from `geometry` (a dict as in
+        bwpm_b200.workloads.geometry_labels); no label volume exists on the host."""
+        from bwpm_b200.geometry import kind_of, params_of
+
+        self = cls.__new__(cls)
+        self._h = None
+        indices = np.ascontiguousarray(indices, dtype=np.complex128).ravel()
+        mask_a = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        prm = params_of(geometry)
+        ib = complex(index_before)
+        self.ny, self.nx, self.nz = int(ny), int(nx), int(geometry["nz"])
+        self.precision = int(precision)
+        h = ctypes.c_void_p()
+        check(lib.bwpm_solver_create_geometry(
+            self.ny, self.nx, float(dy), float(dx), float(dz), float(k0), ptr(indices),
+            indices.size, kind_of(geometry), ptr(prm), prm.size, self.nz, ib.real, ib.imag,
+            ptr(mask_a), int(device), self.precision, ctypes.byref(h)))
+        self._h = h
+        return self
 
     def __del__(self):
         if getattr(self, "_h", None):

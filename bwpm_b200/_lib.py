@@ -38,6 +38,9 @@ SIGNATURES: dict[str, tuple] = {
     "bwpm_longitudinal_wavenumber": (_i, [_d, _d, _d, _p, _sz, _p]),
     "bwpm_solver_create": (_i, [_sz, _sz, _d, _d, _d, _d, _p, _sz, _p, _sz, _d, _d, _p, _i, _p,
                                 _i, _d, ctypes.POINTER(_p)]),
+    "bwpm_solver_create_geometry": (_i, [_sz, _sz, _d, _d, _d, _d, _p, _sz, _i, _p, _sz, _sz, _d,
+                                         _d, _p, _i, _i, ctypes.POINTER(_p)]),
+    "bwpm_geometry_labels": (_i, [_i, _i, _p, _sz, _sz, _sz, _sz, _d, _d, _d, _p]),
     "bwpm_solver_run": (_i, [_p, _p, _i, _p, _sz, _p, _p, _p, _p, _p, _p, _i64p]),
     "bwpm_solver_stats": (_i, [_p, _i64p, _i64p, _i64p]),
     "bwpm_solver_destroy": (None, [_p]),
@@ -64,6 +67,8 @@ SIGNATURES: dict[str, tuple] = {
                                             _i, _i64p]),
     "bwpm_server_submit_3d_borrowed": (_i, [_p, _sz, _sz, _d, _d, _d, _d, _p, _sz, _p, _sz, _d, _d,
                                             _p, _p, _i, _i64p]),
+    "bwpm_server_submit_3d_geometry": (_i, [_p, _sz, _sz, _d, _d, _d, _d, _p, _sz, _i, _p, _sz,
+                                            _sz, _d, _d, _p, _p, _i, _i64p]),
     "bwpm_server_wait": (_i, [_p, ctypes.c_int64, _d, ctypes.POINTER(_i)]),
     "bwpm_server_result": (_i, [_p, ctypes.c_int64, _p, _p, _p, _p, _p, _p, _p, _p]),
     "bwpm_server_stats": (_i, [_p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),

@@ -7,6 +7,7 @@
 #include "../../include/bwpm_b200.h"
 #include "batch2d.hpp"
 #include "devbuf.hpp"
+#include "geometry.cuh"
 #include "noalloc.hpp"
 #include "postproc.hpp"
 #include "server.hpp"
@@ -47,6 +48,15 @@ int guarded(F&& f) {
 }
 
 const bwpm::cd* as_cd(const double* p) { return reinterpret_cast<const bwpm::cd*>(p); }
+
+// a stream of the call's own on `device`
+struct CallStream {
+  bwpm::OwnedStream s;
+  explicit CallStream(int device) {
+    bwpm::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    s.create();
+  }
+};
 bwpm::cd* as_cd(double* p) { return reinterpret_cast<bwpm::cd*>(p); }
 
 }  // namespace
@@ -162,6 +172,47 @@ int bwpm_solver_create(size_t ny, size_t nx, double dy, double dx, double dz, do
     auto s = std::make_unique<bwpm_solver>();
     s->impl = bwpm::make_plane_solver(std::move(in), precision);
     *out = s.release();
+  });
+}
+
+int bwpm_solver_create_geometry(size_t ny, size_t nx, double dy, double dx, double dz, double k0,
+                                const double* indices, size_t m, int kind, const double* params,
+                                size_t nparams, size_t nz, double ib_re, double ib_im,
+                                const double* mask, int device, int precision, bwpm_solver** out) {
+  return guarded([&] {
+    if (!out) throw bwpm::invalid_argument("null output handle");
+    *out = nullptr;
+    if (!indices || !params) throw bwpm::invalid_argument("null array");
+    bwpm::SolverInput in;
+    in.ny = ny;
+    in.nx = nx;
+    in.dy = dy;
+    in.dx = dx;
+    in.dz = dz;
+    in.k0 = k0;
+    in.indices.assign(as_cd(indices), as_cd(indices) + m);
+    in.geometry_kind = kind;
+    in.geometry_params.assign(params, params + nparams);
+    in.nz = nz;
+    in.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) in.mask.assign(mask, mask + ny * nx);
+    in.device = device;
+    auto s = std::make_unique<bwpm_solver>();
+    s->impl = bwpm::make_plane_solver(std::move(in), precision);
+    *out = s.release();
+  });
+}
+
+int bwpm_geometry_labels(int device, int kind, const double* params, size_t nparams, size_t nz,
+                         size_t ny, size_t nx, double dz, double dy, double dx, uint8_t* labels) {
+  return guarded([&] {
+    if (!labels) throw bwpm::invalid_argument("null array");
+    const bwpm::GeometrySpec g = bwpm::geometry_spec(kind, params, nparams, nz, ny, nx, dz, dy, dx);
+    CallStream cs(device);
+    bwpm::DevBuf<uint8_t> d(nz * ny * nx, cs.s);
+    bwpm::generate_labels(g, d.ptr, cs.s);
+    bwpm::check_cuda(cudaMemcpyAsync(labels, d.ptr, d.bytes(), cudaMemcpyDeviceToHost, cs.s), "download");
+    bwpm::check_cuda(cudaStreamSynchronize(cs.s), "synchronize");
   });
 }
 
@@ -384,6 +435,35 @@ int bwpm_server_submit_3d_borrowed(bwpm_server* s, size_t ny, size_t nx, double 
                           field, iterations, ticket, true);
 }
 
+int bwpm_server_submit_3d_geometry(bwpm_server* s, size_t ny, size_t nx, double dy, double dx,
+                                   double dz, double k0, const double* indices, size_t m, int kind,
+                                   const double* params, size_t nparams, size_t nz, double ib_re,
+                                   double ib_im, const double* mask, const double* field,
+                                   int iterations, int64_t* ticket) {
+  return guarded([&] {
+    if (!s || !s->impl) throw bwpm::invalid_argument("null server");
+    if (!indices || !params || !field) throw bwpm::invalid_argument("null array");
+    // validated here, so that a bad geometry fails the call rather than the request
+    (void)bwpm::geometry_spec(kind, params, nparams, nz, ny, nx, dz, dy, dx);
+    bwpm::SolverInput in;
+    in.ny = ny;
+    in.nx = nx;
+    in.dy = dy;
+    in.dx = dx;
+    in.dz = dz;
+    in.k0 = k0;
+    in.indices.assign(as_cd(indices), as_cd(indices) + m);
+    in.geometry_kind = kind;
+    in.geometry_params.assign(params, params + nparams);
+    in.nz = nz;
+    in.index_before = bwpm::cd{ib_re, ib_im};
+    if (mask) in.mask.assign(mask, mask + ny * nx);
+    std::vector<bwpm::cd> f(as_cd(field), as_cd(field) + 2 * ny * nx);
+    const int64_t k = s->impl->submit3d(std::move(in), std::move(f), iterations, nullptr);
+    if (ticket) *ticket = k;
+  });
+}
+
 int bwpm_server_wait(bwpm_server* s, int64_t ticket, double timeout_s, int* done) {
   return guarded([&] {
     if (!s || !s->impl) throw bwpm::invalid_argument("null server");
@@ -443,14 +523,6 @@ bwpm::PlaneGeometry plane_geometry(size_t ny, size_t nx, double dy, double dx, d
   return g;
 }
 
-// a stream of the call's own on `device`
-struct CallStream {
-  bwpm::OwnedStream s;
-  explicit CallStream(int device) {
-    bwpm::check_cuda(cudaSetDevice(device), "cudaSetDevice");
-    s.create();
-  }
-};
 }  // namespace
 
 int bwpm_port_power(int device, size_t ny, size_t nx, double dy, double dx, double k0,

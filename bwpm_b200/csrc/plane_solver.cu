@@ -19,6 +19,7 @@
 
 #include "born_kernels.cuh"
 #include "devbuf.hpp"
+#include "geometry.cuh"
 #include "plan.hpp"
 #include "plane_kernels.cuh"
 #include "plane_setup.cuh"
@@ -161,9 +162,12 @@ void PlaneSolver<T>::setup() {
   const std::size_t nn = n();
   if (in_.ny < 1 || in_.nx < 1) throw invalid_argument("ny and nx must be positive");
   const std::int32_t* labels = in_.labels_view ? in_.labels_view : in_.labels.data();
-  if (in_.labels_device) {  // uint8 labels on the device (generated there; in range by construction)
+  if (in_.labels_device || in_.geometry_kind >= 0) {  // uint8 labels on the device (in range)
     if (in_.indices.size() > 255) throw invalid_argument("device labels take at most 255 materials");
     if (!in_.fluct.empty()) throw invalid_argument("fluctuation needs host labels");
+    if (in_.geometry_kind >= 0 &&
+        in_.indices.size() < static_cast<std::size_t>(geometry_materials(in_.geometry_kind)))
+      throw invalid_argument("labels must index into `indices`");
     labels = nullptr;
   } else if (!in_.labels_view && in_.labels.size() != in_.nz * nn) {
     throw invalid_argument("labels must have shape (nz, ny, nx)");
@@ -219,6 +223,15 @@ void PlaneSolver<T>::setup() {
   upload_tw(hy_, tw_y_);
   upload_tw(hx_, tw_x_);
 
+  DevBuf<std::uint8_t> generated;  // labels generated from a geometry, freed after set-up
+  if (in_.geometry_kind >= 0) {
+    const GeometrySpec g = geometry_spec(in_.geometry_kind, in_.geometry_params.data(),
+                                         in_.geometry_params.size(), in_.nz, in_.ny, in_.nx,
+                                         in_.dz, in_.dy, in_.dx);
+    generated.alloc(std::max<std::size_t>(1, in_.nz * nn), stream_);
+    generate_labels(g, generated.ptr, stream_);
+    in_.labels_device = generated.ptr;
+  }
   // per-step pairs, pair-id planes and interface lists: on the device for large volumes (or
   // labels already on the device), else on the host (pair-id planes deduplicated); the
   // environment variable BWPM_SETUP=host|device overrides the choice where both can run

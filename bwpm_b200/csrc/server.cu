@@ -63,10 +63,12 @@ struct Group {
 };
 
 // Device memory of a complex64 3D solve: field planes and work planes (≈ 10 planes of
-// ny·nx·2 complex64), operator tables (48 B per point each, about 16 for two materials), pair ids.
+// ny·nx·2 complex64), operator tables (48 B per point each, about 16 for two materials), and
+// during set-up the uint8 label volume and pair-id planes (at most one byte per point and slab
+// each).
 std::size_t estimate_3d_bytes(const SolverInput& in) {
   const std::size_t n = in.ny * in.nx;
-  return n * (16 * 10 + 48 * 16) + in.nz * n / 4;
+  return n * (16 * 10 + 48 * 16) + 2 * in.nz * n;
 }
 
 class ServerImpl final : public Server {

@@ -23,6 +23,10 @@ struct SolverInput {
   // or, when set, uint8 labels in device memory (nz·ny·nx values on `device`, e.g. generated
   // there from a geometry), read during set-up only; at most 255 materials, no fluctuation
   const std::uint8_t* labels_device = nullptr;
+  // or, when geometry_kind ≥ 0, labels generated on the device from that geometry during
+  // set-up (see generate_labels): kGeometryParams values in geometry_params
+  int geometry_kind = -1;
+  std::vector<double> geometry_params;
   std::size_t nz = 0;
   cd index_before{1.0, 0.0};
   std::vector<double> mask;          // (ny, nx) or empty
@@ -55,6 +59,18 @@ class Solver {
 
 // precision: 64 (complex128 fields, the drop-in path) or 32 (complex64 fields, FP64 tables).
 std::unique_ptr<Solver> make_plane_solver(SolverInput in, int precision);
+
+// Geometry of a label volume generated on the device (geometry.cuh): kind (0 tilted facet,
+// 1 lens array, 2 microlens, 3 tilted slab) and kGeometryParams parameters
+// (base, tan_tilt, pitch, sag, radius, vertex, back).
+constexpr std::size_t kGeometryParams = 7;
+struct GeometrySpec;
+GeometrySpec geometry_spec(int kind, const double* params, std::size_t nparams, std::size_t nz,
+                           std::size_t ny, std::size_t nx, double dz, double dy, double dx);
+// materials a geometry labels (labels 0 … n − 1)
+int geometry_materials(int kind);
+// uint8 labels (nz, ny, nx) into device memory `out`, on `stream`
+void generate_labels(const GeometrySpec& g, std::uint8_t* out, cudaStream_t stream);
 
 // Interface matrices on the device for n points (kind 0: T, 1: R), out (n, 2, 2) complex128.
 void interface_matrices(int reflection, const double* kx, const double* ky, std::size_t n, cd n_in,

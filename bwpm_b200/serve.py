@@ -53,20 +53,32 @@ class Server:
 
     def submit(self, prob, borrow: bool = True) -> int:
         """Submits a `bwpm_b200.workloads.Problem` (nx = 1: 2D, else 3D); returns its ticket.
+        A 3D problem with `labels` None and a `geometry` has its labels generated on the device.
 
         borrow: the server takes the labels after the call returns (2D: copied by a preparation
         worker, 3D: read in place by the set-up; the Server holds the array until the request's
         result is taken), so a large 3D submission does not stall the caller; False copies
         everything inside the call."""
-        labels = np.ascontiguousarray(prob.labels, dtype=np.int32)
         indices = np.ascontiguousarray(prob.indices, dtype=np.complex128).ravel()
         field = np.ascontiguousarray(prob.field, dtype=np.complex128)
         mask = None if prob.mask is None else np.ascontiguousarray(prob.mask, dtype=np.float64)
         ib = complex(prob.index_before)
-        nz = labels.shape[0]
         t = ctypes.c_int64()
         if prob.fluctuation is not None:
             raise ValueError("the server takes problems without a fluctuation term")
+        if prob.nx != 1 and prob.labels is None and prob.geometry is not None:
+            # 3D without a label volume: labels generated on the device from the geometry
+            from bwpm_b200.geometry import kind_of, params_of
+
+            prm = params_of(prob.geometry)
+            check(lib.bwpm_server_submit_3d_geometry(
+                self._h, prob.ny, prob.nx, prob.dy, prob.dx, prob.dz, prob.k0, ptr(indices),
+                indices.size, kind_of(prob.geometry), ptr(prm), prm.size, prob.nz, ib.real,
+                ib.imag, ptr(mask), ptr(field), int(prob.iterations), ctypes.byref(t)))
+            self._shape[t.value] = (prob.ny, prob.nx, int(prob.iterations), True)
+            return int(t.value)
+        labels = np.ascontiguousarray(prob.ensure_labels(), dtype=np.int32)
+        nz = labels.shape[0]
         if prob.nx == 1:
             fn = lib.bwpm_server_submit_2d_borrowed if borrow else lib.bwpm_server_submit_2d
             check(fn(self._h, prob.ny, prob.dy, prob.dz, prob.k0, ptr(indices), indices.size,

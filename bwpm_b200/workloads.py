@@ -50,6 +50,56 @@ def absorbing_mask_1d(coords: np.ndarray, width: float, order: int = 8,
     return np.asarray(edge ** (u**order), dtype=np.float64)
 
 
+GEOMETRY_KINDS = ("tilted_facet", "lens_array", "microlens", "tilted_slab")
+
+
+def geometry_labels(g: dict) -> np.ndarray:
+    """uint8 labels (nz, ny, nx) of a geometry at the pixel centres (the rule of
+    src/bwpm/geometry.py:24-37: slab j at z = (j + 0.5)·dz, centred lateral grid). The same FP64
+    operations in the same order as the device generator (csrc/geometry.cuh), so both give
+    identical labels. Keys: kind, nz, ny, nx, dz, dy, dx and per kind
+    - tilted_facet: base, tan_tilt (label 1 where z ≥ base + tan_tilt·y);
+    - lens_array: base, pitch, sag, radius (label 1 where z ≥ base − h(x, y), spherical caps);
+    - microlens: vertex, radius, back, tan_tilt (1 inside the cap, 2 behind the tilted face);
+    - tilted_slab: base, tan_tilt, back (1 where base + tan_tilt·y ≤ z < back)."""
+    nz, ny, nx = int(g["nz"]), int(g["ny"]), int(g["nx"])
+    z = (np.arange(nz) + 0.5) * g["dz"]
+    y = centred(ny, g["dy"])
+    x = centred(nx, g["dx"])
+    zz = z[:, None, None]
+    kind = g["kind"]
+    if kind == "tilted_facet":
+        surface = g["base"] + g["tan_tilt"] * y[:, None] * np.ones((1, nx))
+        return (zz >= surface[None]).astype(np.uint8)
+    if kind == "lens_array":
+        half = g["pitch"] / 2
+        coords = [y[:, None] * np.ones((1, nx))]
+        if nx > 1:
+            coords.append(x[None, :] * np.ones((ny, 1)))
+        r2 = 0.0
+        for c in coords:
+            local = (c + half) % g["pitch"] - half
+            r2 = r2 + local**2
+        height = np.sqrt(np.maximum(g["radius"] ** 2 - r2, 0.0)) - (g["radius"] - g["sag"])
+        height = np.maximum(height, 0.0)
+        return (zz >= (g["base"] - height)[None]).astype(np.uint8)
+    if kind == "microlens":
+        r2 = x[None, :] ** 2 + y[:, None] ** 2
+        radius = g["radius"]
+        sag = g["vertex"] + radius - np.sqrt(np.maximum(radius**2 - r2, 0.0))
+        sag = np.where(r2 < radius**2, sag, np.inf)
+        back_face = g["back"] + g["tan_tilt"] * y[:, None] * np.ones((1, nx))
+        labels = np.zeros((nz, ny, nx), dtype=np.uint8)
+        labels[zz >= sag[None]] = 1
+        labels[zz >= back_face[None]] = 2
+        return labels
+    if kind == "tilted_slab":
+        front = g["base"] + g["tan_tilt"] * y
+        glass = (z[:, None] >= front[None, :]) & (z[:, None] < g["back"])
+        return np.repeat(glass.astype(np.uint8)[:, :, None], nx, axis=2)
+    raise ValueError(f"unknown geometry kind {kind!r}")
+
+
 @dataclass
 class Problem:
     """One solve: geometry, materials, incident field and iteration count."""
@@ -61,7 +111,7 @@ class Problem:
     dz: float
     k0: float
     indices: np.ndarray          # complex128 (M,)
-    labels: np.ndarray           # int32 (nz, ny, nx)
+    labels: np.ndarray | None    # int32 (nz, ny, nx), or None when `geometry` describes them
     index_before: complex
     mask: np.ndarray | None      # float64 (ny, nx) or None
     field: np.ndarray            # complex128 (ny, nx, 2)
@@ -69,21 +119,29 @@ class Problem:
     fluctuation: np.ndarray | None = None  # complex128 (nz, ny, nx) or None
     name: str = ""
     extra: dict = field(default_factory=dict)
+    geometry: dict | None = None  # the body the labels come from (see geometry_labels)
 
     @property
     def nz(self) -> int:
-        return int(self.labels.shape[0])
+        return int(self.labels.shape[0]) if self.labels is not None else int(self.geometry["nz"])
+
+    def ensure_labels(self) -> np.ndarray:
+        """The int32 labels, generated on the host from `geometry` when not stored."""
+        if self.labels is None:
+            self.labels = geometry_labels(self.geometry).astype(np.int32)
+        return self.labels
 
     def core_args(self) -> tuple:
         """Positional constructor arguments of bwpm._core.Solver / CudaSolver."""
-        return (self.ny, self.nx, self.dy, self.dx, self.dz, self.k0, self.indices, self.labels,
+        return (self.ny, self.nx, self.dy, self.dx, self.dz, self.k0, self.indices,
+                self.ensure_labels(),
                 complex(self.index_before), self.mask)
 
     def arrays(self) -> dict[str, np.ndarray]:
         out = {
             "grid": np.array([self.ny, self.nx, self.dy, self.dx, self.dz, self.k0]),
             "indices": self.indices,
-            "labels": self.labels,
+            "labels": self.ensure_labels(),
             "index_before": np.array(complex(self.index_before)),
             "field": self.field,
             "iterations": np.array(self.iterations),
@@ -185,20 +243,16 @@ def microlens3d(n: int = 512, nz: int = 400, iterations: int = 6,
     back = 24e-3 * sz
     x = centred(n, dx)
     y = centred(n, dy)
-    z = (np.arange(nz) + 0.5) * dz
     r2 = x[None, :] ** 2 + y[:, None] ** 2
-    sag = vertex + radius - np.sqrt(np.maximum(radius**2 - r2, 0.0))
-    sag = np.where(r2 < radius**2, sag, np.inf)
-    back_face = back + np.tan(np.deg2rad(5.0)) * y[:, None] * np.ones((1, n))
-    zz = z[:, None, None]
-    labels = np.zeros((nz, n, n), dtype=np.int32)
-    labels[zz >= sag[None]] = 1
-    labels[zz >= back_face[None]] = 2
+    geometry = {"kind": "microlens", "nz": nz, "ny": n, "nx": n, "dz": dz, "dy": dy, "dx": dx,
+                "vertex": vertex, "radius": radius, "back": back,
+                "tan_tilt": float(np.tan(np.deg2rad(5.0)))}
+    labels = geometry_labels(geometry).astype(np.int32)
     mask = absorbing_mask_1d(y, 16 * dy)[:, None] * absorbing_mask_1d(x, 16 * dx)[None, :]
     prof = np.exp(-r2 / (8e-3 * max(sr, 0.1)) ** 2).astype(np.complex128)
     return Problem(n, n, dy, dx, dz, k0_of(wavelength_um),
                    np.array([1.0 + 0j, 1.52 + 0j, SILVER_CFG3]), labels, 1.0 + 0j, mask,
-                   _vec(prof, "te"), iterations, name=f"microlens3d_{n}")
+                   _vec(prof, "te"), iterations, name=f"microlens3d_{n}", geometry=geometry)
 
 
 def tilted_slab2d_params(rng: np.random.Generator, i: int, sizes=BATCH_SIZES,
@@ -226,18 +280,16 @@ def tilted_slab2d_from(prm: dict) -> Problem:
     dy, dz = lam / 8, lam / 10
     k0 = k0_of(wl)
     y = centred(ny, dy)
-    z = (np.arange(nz) + 0.5) * dz
-    front = nz // 4 * dz + np.tan(tilt) * y
-    back = (3 * nz) // 4 * dz
-    glass = (z[:, None] >= front[None, :]) & (z[:, None] < back)
-    labels = glass.astype(np.int32)[:, :, None]
+    geometry = {"kind": "tilted_slab", "nz": nz, "ny": ny, "nx": 1, "dz": dz, "dy": dy, "dx": 1.0,
+                "base": nz // 4 * dz, "tan_tilt": float(np.tan(tilt)), "back": (3 * nz) // 4 * dz}
+    labels = geometry_labels(geometry).astype(np.int32)
     w0 = ny * dy / 8
     prof = (np.exp(-((y / w0) ** 2)) * np.exp(1j * k0 * np.sin(theta) * y))[:, None]
     mask = absorbing_mask_1d(y, ny * dy / 10)[:, None]
     pol = "te" if i % 2 == 0 else "tm"
     return Problem(ny, 1, dy, 1.0, dz, k0, np.array([1.0 + 0j, n + 0j]), labels, 1.0 + 0j, mask,
                    _vec(prof, pol), iterations, name=f"batch2d_{i}_{pol}",
-                   extra={"wavelength_um": wl, "theta": theta, "tilt": tilt})
+                   extra={"wavelength_um": wl, "theta": theta, "tilt": tilt}, geometry=geometry)
 
 
 def batch2d_params(count: int = 256, seed: int = 4, sizes=BATCH_SIZES, nz_range=(100, 2000),
@@ -266,28 +318,15 @@ def smooth_sizes(lo: int, hi: int) -> list[int]:
     return out
 
 
-def _lens_array_profile(rng: np.random.Generator, coords: list[np.ndarray]) -> tuple:
-    pitch = float(rng.uniform(20e-3, 60e-3))
-    sag = float(rng.uniform(2e-3, 10e-3))
-    n = float(rng.uniform(1.46, 1.6))
-    # each lenslet is a spherical cap of height `sag` over half the pitch
-    half = pitch / 2
-    radius = (half**2 + sag**2) / (2 * sag)
-    r2 = 0.0
-    for c in coords:
-        local = (c + half) % pitch - half
-        r2 = r2 + local**2
-    height = np.sqrt(np.maximum(radius**2 - r2, 0.0)) - (radius - sag)
-    return np.maximum(height, 0.0), n
-
-
 SERVED_3D_LATERAL = (256, 384, 512, 768, 1024)
 
 
 def request(rng: np.random.Generator, i: int, iterations: int = 2,
-            max_lateral_3d: int = 1024) -> Problem:
+            max_lateral_3d: int = 1024, host_labels: bool = True) -> Problem:
     """One request of the served stream: 70 % 2D, 30 % 3D; microlens array or tilted facet.
-    3D lateral sizes are drawn from SERVED_3D_LATERAL up to `max_lateral_3d`."""
+    3D lateral sizes are drawn from SERVED_3D_LATERAL up to `max_lateral_3d`. The body is kept
+    as `geometry`; with host_labels=False a 3D request carries no label volume (labels = None:
+    they are generated where they are used, e.g. on the device)."""
     is2d = rng.uniform() < 0.7
     wl = 0.633
     lam = wl * 1e-3
@@ -296,52 +335,56 @@ def request(rng: np.random.Generator, i: int, iterations: int = 2,
         ny, nx = int(rng.choice(smooth_sizes(1024, 4096))), 1
         nz = int(rng.integers(500, 2001))
         dy, dx, dz = lam / 8, 1.0, lam / 10
-        y = centred(ny, dy)
-        coords = [y[:, None] * np.ones((1, 1))]
     else:
         ny = nx = int(rng.choice([v for v in SERVED_3D_LATERAL if v <= max_lateral_3d]))
         nz = int(rng.integers(200, 601))
         dy = dx = lam / 6
         dz = lam / 8
-        y = centred(ny, dy)
-        x = centred(nx, dx)
-        coords = [y[:, None] * np.ones((1, nx)), x[None, :] * np.ones((ny, 1))]
-    z = (np.arange(nz) + 0.5) * dz
-    base = nz // 3 * dz
+    y = centred(ny, dy)
+    x = centred(nx, dx)
+    geometry = {"nz": nz, "ny": ny, "nx": nx, "dz": dz, "dy": dy, "dx": dx,
+                "base": nz // 3 * dz}
     if rng.uniform() < 0.5:
-        height, n = _lens_array_profile(rng, coords)
-        surface = base - height  # lenslets bulge toward −z from the substrate at `base`
+        # a square array of spherical caps of height `sag` over half the pitch, bulging toward
+        # −z from the substrate at `base`
+        pitch = float(rng.uniform(20e-3, 60e-3))
+        sag = float(rng.uniform(2e-3, 10e-3))
+        n = float(rng.uniform(1.46, 1.6))
+        half = pitch / 2
+        geometry.update(kind="lens_array", pitch=pitch, sag=sag,
+                        radius=(half**2 + sag**2) / (2 * sag))
         kind = "lens_array"
     else:
         n = float(rng.uniform(1.44, 1.47))
         tilt = float(rng.uniform(0.0, np.deg2rad(8.0)))
-        surface = base + np.tan(tilt) * coords[0]
+        geometry.update(kind="tilted_facet", tan_tilt=float(np.tan(tilt)))
         kind = "fiber_facet"
-    labels = (z[:, None, None] >= surface[None]).astype(np.int32)
+    labels = geometry_labels(geometry).astype(np.int32) if (host_labels or is2d) else None
     if is2d:
         w0 = ny * dy / 8
         prof = np.exp(-((y / w0) ** 2))[:, None]
         mask = absorbing_mask_1d(y, ny * dy / 10)[:, None]
     else:
         w0 = ny * dy / 8
-        r2 = coords[0] ** 2 + coords[1] ** 2
+        r2 = (y[:, None] * np.ones((1, nx))) ** 2 + (x[None, :] * np.ones((ny, 1))) ** 2
         prof = np.exp(-r2 / w0**2)
         mask = absorbing_mask_1d(y, ny * dy / 10)[:, None] * absorbing_mask_1d(x, nx * dx / 10)[None, :]
     pol = "te" if rng.uniform() < 0.5 else "tm"
     return Problem(ny, nx, dy, dx, dz, k0, np.array([1.0 + 0j, n + 0j]), labels, 1.0 + 0j, mask,
                    _vec(prof.astype(np.complex128), pol), iterations,
-                   name=f"request_{i}_{kind}_{'2d' if is2d else '3d'}")
+                   name=f"request_{i}_{kind}_{'2d' if is2d else '3d'}", geometry=geometry)
 
 
 def request_stream(count: int, rate_hz: float, seed: int = 5, iterations: int = 2,
-                   max_lateral_3d: int = 1024) -> list[tuple[float, Problem]]:
+                   max_lateral_3d: int = 1024,
+                   host_labels: bool = True) -> list[tuple[float, Problem]]:
     """Seeded Poisson arrivals: (arrival time in s, problem)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(count):
         t += float(rng.exponential(1.0 / rate_hz))
-        out.append((t, request(rng, i, iterations, max_lateral_3d)))
+        out.append((t, request(rng, i, iterations, max_lateral_3d, host_labels)))
     return out
 
 

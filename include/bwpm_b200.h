@@ -182,6 +182,15 @@ int bwpm_server_submit_3d_borrowed(bwpm_server* s, size_t ny, size_t nx, double 
                                    double index_before_im, const double* mask,
                                    const double* field, int iterations, int64_t* ticket);
 
+/* A 3D request whose labels are generated on the device from a geometry (see
+ * bwpm_geometry_labels): no label volume is passed or held on the host. */
+int bwpm_server_submit_3d_geometry(bwpm_server* s, size_t ny, size_t nx, double dy, double dx,
+                                   double dz, double k0, const double* indices, size_t m, int kind,
+                                   const double* params, size_t nparams, size_t nz,
+                                   double index_before_re, double index_before_im,
+                                   const double* mask, const double* field, int iterations,
+                                   int64_t* ticket);
+
 /* Waits up to timeout_s seconds (< 0: without limit); *done = 1 when the request finished. */
 int bwpm_server_wait(bwpm_server* s, int64_t ticket, double timeout_s, int* done);
 
@@ -198,6 +207,37 @@ int bwpm_server_stats(bwpm_server* s, int64_t* submitted, int64_t* completed, in
                       int64_t* kernel_launches, int64_t* max_concurrent);
 
 void bwpm_server_destroy(bwpm_server* s);
+
+/* ---- label volumes generated on the device from a geometry -----------------------------------
+ * The labelling rule of the reference's bwpm.geometry.labels_at_centres
+ * (src/bwpm/geometry.py:24-37): slab j takes the material at its centre z = (j + 0.5)·dz, on the
+ * centred lateral grid y_i = (i − ny//2)·dy, x_k = (k − nx//2)·dx. The reference takes a Python
+ * predicate for the body; these entry points take one of four parametrised bodies and write
+ * uint8 labels straight into device memory, so a large volume never exists on the host.
+ * params (BWPM_GEOMETRY_PARAMS doubles, mm): base, tan_tilt, pitch, sag, radius, vertex, back.
+ *   TILTED_FACET: 1 where z ≥ base + tan_tilt·y, else 0.
+ *   LENS_ARRAY:   1 where z ≥ base − h(x, y), h = max(√(radius² − r²) − (radius − sag), 0) with
+ *                 r the distance to the nearest lenslet centre of a square array of `pitch`.
+ *   MICROLENS:    1 where r² < radius² and z ≥ vertex + radius − √(radius² − r²); 2 where
+ *                 z ≥ back + tan_tilt·y (takes precedence); else 0.
+ *   TILTED_SLAB:  1 where base + tan_tilt·y ≤ z < back, else 0. */
+#define BWPM_GEOMETRY_TILTED_FACET 0
+#define BWPM_GEOMETRY_LENS_ARRAY 1
+#define BWPM_GEOMETRY_MICROLENS 2
+#define BWPM_GEOMETRY_TILTED_SLAB 3
+#define BWPM_GEOMETRY_PARAMS 7
+
+/* Generates the labels (nz·ny·nx uint8) on `device` and copies them to host `labels`. */
+int bwpm_geometry_labels(int device, int kind, const double* params, size_t nparams, size_t nz,
+                         size_t ny, size_t nx, double dz, double dy, double dx, uint8_t* labels);
+
+/* bwpm_solver_create with the labels generated on the device from a geometry (no label volume
+ * on the host; the per-step tables are built on the device too). No fluctuation. */
+int bwpm_solver_create_geometry(size_t ny, size_t nx, double dy, double dx, double dz, double k0,
+                                const double* indices, size_t m, int kind, const double* params,
+                                size_t nparams, size_t nz, double index_before_re,
+                                double index_before_im, const double* mask, int device,
+                                int precision, bwpm_solver** out);
 
 /* ---- post-processing of fields on the device (FP64, compensated sums) ----------------------
  * `field`: host complex128 (ny, nx, 2) (E_x, E_y) on the centred grid; k grids of
