@@ -142,30 +142,6 @@ __global__ void k_axpby(cx<T>* y, const cx<T>* x, cd a, cd b, long long m) {
   y[i] = cast<T>(a * cast<double>(x[i]) + b * cast<double>(y[i]));
 }
 
-// partial[block] = Σ conj(u)·v over the block's range, accumulated in FP64.
-template <typename T>
-__global__ void k_dot_partial(const cx<T>* u, const cx<T>* v, long long m, cd* partial) {
-  __shared__ cd red[32];
-  cd acc{0.0, 0.0};
-  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < m;
-       i += static_cast<long long>(gridDim.x) * blockDim.x)
-    acc = acc + conj(cast<double>(u[i])) * cast<double>(v[i]);
-  for (int o = 16; o > 0; o >>= 1) {
-    acc.re += __shfl_down_sync(0xffffffffu, acc.re, o);
-    acc.im += __shfl_down_sync(0xffffffffu, acc.im, o);
-  }
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    acc = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : cd{0.0, 0.0};
-    for (int o = 16; o > 0; o >>= 1) {
-      acc.re += __shfl_down_sync(0xffffffffu, acc.re, o);
-      acc.im += __shfl_down_sync(0xffffffffu, acc.im, o);
-    }
-    if (threadIdx.x == 0) partial[blockIdx.x] = acc;
-  }
-}
-
 // ---- transforms of planes with ncomp interleaved components ---------------------------------
 
 // nx = 1: one CTA per component, the whole line in shared memory.

@@ -83,6 +83,44 @@ struct DevBuf {
 
 // A non-blocking stream owned by a solver; declared before the solver's buffers so that it is
 // destroyed after them.
+// RAII page-locked host allocation (cudaHostAlloc).
+template <typename U>
+struct PinnedBuf {
+  U* ptr = nullptr;
+  std::size_t n = 0;
+  PinnedBuf() = default;
+  void alloc(std::size_t count) {
+    release();
+    n = count;
+    if (count)
+      check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&ptr), count * sizeof(U), cudaHostAllocDefault),
+                 "cudaHostAlloc");
+  }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  ~PinnedBuf() { release(); }
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+};
+
+// RAII CUDA event without timing.
+struct OwnedEvent {
+  cudaEvent_t e = nullptr;
+  OwnedEvent() = default;
+  void create() {
+    if (!e) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  ~OwnedEvent() {
+    if (e) cudaEventDestroy(e);
+  }
+  OwnedEvent(const OwnedEvent&) = delete;
+  OwnedEvent& operator=(const OwnedEvent&) = delete;
+  operator cudaEvent_t() const { return e; }
+};
+
 struct OwnedStream {
   cudaStream_t s = nullptr;
   OwnedStream() = default;

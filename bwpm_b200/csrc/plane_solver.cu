@@ -20,6 +20,7 @@
 #include "born_kernels.cuh"
 #include "devbuf.hpp"
 #include "geometry.cuh"
+#include "gmres_kernels.cuh"
 #include "plan.hpp"
 #include "plane_kernels.cuh"
 #include "plane_setup.cuh"
@@ -76,7 +77,6 @@ class PlaneSolver final : public Solver {
   // the forward/backward sweeps of a run (device work only, unless Born slabs need GMRES)
   void sweeps(int iterations, const std::vector<int>& keep_slot, DevBuf<C>& kept_f, DevBuf<C>& kept_b,
               DevBuf<C>& t_iter, DevBuf<C>& r_iter);
-  cd dot(const C* u, const C* v, long long m);
   void axpby(C* y, const C* x, cd a, cd b, long long m);
   void add_plane_scaled(C* dst, const C* src, const T* mask);
   LaunchShape rows_shape(int ncomp, int rows_max) const;
@@ -117,8 +117,10 @@ class PlaneSolver final : public Solver {
   DevBuf<C> pot_, born_fwd_, born_bwd_, w3_, t3_, sources_, g_x_, g_rhs_, g_y_, g_w_, g_tmp_,
       inc_;
   std::vector<DevBuf<C>> basis_;
-  DevBuf<cd> partial_;
-  std::vector<cd> partial_host_;
+  DevBuf<GmresState> gst_;
+  DevBuf<cd> dot_partial_;
+  PinnedBuf<int> flags_host_;
+  OwnedEvent gmres_events_[kGmresRestart];
   // launch shapes
   int thr2d_ = 32, thr_line3_ = 32;
   int sms_ = 148;
@@ -430,8 +432,6 @@ void PlaneSolver<T>::setup() {
     t3_.alloc(3 * nn, stream_);
     sources_.alloc(6 * nn, stream_);
     for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &inc_}) b->alloc(2 * nn, stream_);
-    partial_.alloc(1024, stream_);
-    partial_host_.resize(1024);
   }
   check_cuda(cudaStreamSynchronize(stream_), "setup");  // this solver's stream only
 }
@@ -679,18 +679,6 @@ void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir) {
 }
 
 template <typename T>
-cd PlaneSolver<T>::dot(const C* u, const C* v, long long m) {
-  const int blocks = static_cast<int>(std::min<long long>(1024, (m + 255) / 256));
-  launch(k_dot_partial<T>, dim3(blocks), dim3(256), 0, u, v, m, partial_.ptr);
-  check_cuda(cudaMemcpyAsync(partial_host_.data(), partial_.ptr, blocks * sizeof(cd),
-                             cudaMemcpyDeviceToHost, stream_), "dot");
-  check_cuda(cudaStreamSynchronize(stream_), "dot");
-  cd s{0.0, 0.0};
-  for (int i = 0; i < blocks; ++i) s = s + partial_host_[i];
-  return s;
-}
-
-template <typename T>
 void PlaneSolver<T>::axpby(C* y, const C* x, cd a, cd b, long long m) {
   launch(k_axpby<T>, dim3(ceil_div(m, kThreads)), dim3(kThreads), 0, y, x, a, b, m);
 }
@@ -703,85 +691,92 @@ void PlaneSolver<T>::add_plane_scaled(C* dst, const C* src, const T* mask) {
          static_cast<T>(1.0 / static_cast<double>(n())), n2);
 }
 
-// GMRES(30) for (1 − G/2)·y = rhs with start y = rhs (cpp/src/solver.cpp:130-207, :336-342).
+// GMRES(30) for (1 − G/2)·y = rhs with start y = rhs (cpp/src/solver.cpp:130-207, :336-342),
+// scalar work on the device (gmres_kernels.cuh). The host waits on the device three times per
+// restart (‖rhs‖ once per solve, β, the final residual) and otherwise only for the convergence
+// flag of the previous Arnoldi step while the next one runs.
 template <typename T>
 void PlaneSolver<T>::gmres(int slot, int dir) {
   const long long m2 = 2 * static_cast<long long>(n());
-  const int restart = 30;
+  constexpr int m = kGmresRestart;
   const double tol = in_.gmres_tol;
-  if (basis_.empty())
-    for (int i = 0; i <= restart; ++i) basis_.emplace_back(static_cast<std::size_t>(m2), stream_);
+  if (basis_.empty()) {
+    for (int i = 0; i <= m; ++i) basis_.emplace_back(static_cast<std::size_t>(m2), stream_);
+    gst_.alloc(1, stream_);
+    check_cuda(cudaMemsetAsync(gst_.ptr, 0, sizeof(GmresState), stream_), "memset");
+    dot_partial_.alloc(kDotBlocks, stream_);
+    flags_host_.alloc(m + 2);
+    for (auto& e : gmres_events_) e.create();
+  }
+  GmresState* st = gst_.ptr;
+  const int vblocks = static_cast<int>(ceil_div(m2, static_cast<long long>(kThreads)));
+  const int dblocks = static_cast<int>(std::min<long long>(kDotBlocks, ceil_div(m2, 256LL)));
+  auto dot_into = [&](const C* u, const C* v, cd* out) {
+    launch(k_dot_dev<T>, dim3(dblocks), dim3(256), 0, u, v, m2, dot_partial_.ptr, &st->counter, out);
+  };
   auto apply = [&](const C* v, C* av) {  // av = v − G v/2
     born_operator(v, g_tmp_.ptr, slot, dir);
     ++gmres_applies_;
     check_cuda(cudaMemcpyAsync(av, v, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
     axpby(av, g_tmp_.ptr, cd{-0.5, 0.0}, cd{1.0, 0.0}, m2);
   };
-  auto norm = [&](const C* u) { return std::sqrt(dot(u, u, m2).re); };
+  auto host_norm = [&](const C* u) {  // ‖u‖ read back on the host
+    dot_into(u, u, &st->dot);
+    cd d;
+    check_cuda(cudaMemcpyAsync(&d, &st->dot, sizeof(cd), cudaMemcpyDeviceToHost, stream_), "dot");
+    check_cuda(cudaStreamSynchronize(stream_), "dot");
+    return std::sqrt(d.re);
+  };
   check_cuda(cudaMemcpyAsync(g_y_.ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
-  const double bnorm = norm(g_rhs_.ptr);
+  const double bnorm = host_norm(g_rhs_.ptr);
   if (bnorm == 0.0) return;
-  const int m = restart;
-  std::vector<cd> h((m + 1) * m), gv(m + 1), cs(m), sn(m);
   for (int outer = 0; outer < 100; ++outer) {
     apply(g_y_.ptr, g_w_.ptr);
     check_cuda(cudaMemcpyAsync(basis_[0].ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
     axpby(basis_[0].ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
-    const double beta = norm(basis_[0].ptr);
+    const double beta = host_norm(basis_[0].ptr);  // leaves the dot in st->dot
     if (beta <= tol * bnorm) return;
-    axpby(basis_[0].ptr, basis_[0].ptr, cd{0.0, 0.0}, cd{1.0 / beta, 0.0}, m2);
-    std::fill(gv.begin(), gv.end(), cd{0.0, 0.0});
-    gv[0] = cd{beta, 0.0};
+    launch(k_norm_scale<T>, dim3(vblocks), dim3(kThreads), 0, basis_[0].ptr, (const C*)basis_[0].ptr,
+           (const cd*)&st->dot, &st->nrm, m2);
+    launch(k_gmres_start, dim3(1), dim3(64), 0, st);
     int used = 0;
     bool done = false;
+    auto converged = [&](int j) {  // waits for the flag of Arnoldi step j
+      check_cuda(cudaEventSynchronize(gmres_events_[j]), "gmres flag");
+      return flags_host_.ptr[j] != 0;
+    };
     for (int j = 0; j < m; ++j) {
       apply(basis_[j].ptr, g_w_.ptr);
-      for (int i = 0; i <= j; ++i) {
-        const cd hij = dot(basis_[i].ptr, g_w_.ptr, m2);
-        h[i * m + j] = hij;
-        axpby(g_w_.ptr, basis_[i].ptr, -hij, cd{1.0, 0.0}, m2);
+      for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, h straight into the Hessenberg matrix
+        dot_into(basis_[i].ptr, g_w_.ptr, &st->h[i * m + j]);
+        launch(k_axpy_dev<T>, dim3(vblocks), dim3(kThreads), 0, g_w_.ptr, (const C*)basis_[i].ptr,
+               (const cd*)&st->h[i * m + j], -1.0, m2);
       }
-      const double hnext = norm(g_w_.ptr);
-      if (hnext > 0.0) {
-        check_cuda(cudaMemcpyAsync(basis_[j + 1].ptr, g_w_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
-        axpby(basis_[j + 1].ptr, basis_[j + 1].ptr, cd{0.0, 0.0}, cd{1.0 / hnext, 0.0}, m2);
-      }
-      for (int i = 0; i < j; ++i) {
-        const cd a = h[i * m + j], c = h[(i + 1) * m + j];
-        h[i * m + j] = cs[i] * a + sn[i] * c;
-        h[(i + 1) * m + j] = -(conj(sn[i]) * a) + cs[i] * c;
-      }
-      const cd a = h[j * m + j];
-      const double aa = std::hypot(a.re, a.im);
-      const double r = std::sqrt(aa * aa + hnext * hnext);
-      if (aa == 0.0) {
-        cs[j] = cd{0.0, 0.0};
-        sn[j] = cd{1.0, 0.0};
-      } else {
-        cs[j] = cd{aa / r, 0.0};
-        sn[j] = (a / aa) * (hnext / r);
-      }
-      h[j * m + j] = cs[j] * a + sn[j] * hnext;
-      gv[j + 1] = -(conj(sn[j]) * gv[j]);
-      gv[j] = cs[j] * gv[j];
-      used = j + 1;
-      if (std::hypot(gv[j + 1].re, gv[j + 1].im) <= tol * bnorm || hnext == 0.0) {
+      dot_into(g_w_.ptr, g_w_.ptr, &st->dot);
+      launch(k_norm_scale<T>, dim3(vblocks), dim3(kThreads), 0, basis_[j + 1].ptr, (const C*)g_w_.ptr,
+             (const cd*)&st->dot, &st->nrm, m2);
+      launch(k_gmres_givens, dim3(1), dim3(32), 0, st, j, tol * bnorm);
+      check_cuda(cudaMemcpyAsync(flags_host_.ptr + j, &st->flag[j], sizeof(int), cudaMemcpyDeviceToHost,
+                                 stream_), "flag");
+      check_cuda(cudaEventRecord(gmres_events_[j], stream_), "event");
+      // step j is queued; the previous step's flag decides whether it counts
+      if (j > 0 && converged(j - 1)) {
+        used = j;
         done = true;
         break;
       }
+      used = j + 1;
     }
-    std::vector<cd> y(used);
-    for (int i = used - 1; i >= 0; --i) {
-      cd s = gv[i];
-      for (int k = i + 1; k < used; ++k) s = s - h[i * m + k] * y[k];
-      y[i] = cdiv(s, h[i * m + i]);
-    }
-    for (int i = 0; i < used; ++i) axpby(g_y_.ptr, basis_[i].ptr, y[i], cd{1.0, 0.0}, m2);
+    if (!done && converged(used - 1)) done = true;
+    launch(k_gmres_backsolve, dim3(1), dim3(32), 0, st, used);
+    for (int i = 0; i < used; ++i)
+      launch(k_axpy_dev<T>, dim3(vblocks), dim3(kThreads), 0, g_y_.ptr, (const C*)basis_[i].ptr,
+             (const cd*)&st->y[i], 1.0, m2);
     if (done) {
       apply(g_y_.ptr, g_w_.ptr);
       check_cuda(cudaMemcpyAsync(g_tmp_.ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
       axpby(g_tmp_.ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
-      if (norm(g_tmp_.ptr) <= tol * bnorm * 10.0) return;
+      if (host_norm(g_tmp_.ptr) <= tol * bnorm * 10.0) return;
     }
   }
   throw std::runtime_error("GMRES did not converge in the Born step (CUDA)");
