@@ -51,12 +51,14 @@ constexpr int table_blocks() {
   return sizeof(T) == sizeof(double) ? 3 : 6;
 }
 
-// Pass j of a step: pair index (into the step's pair-id plane), operator table, reflection flag.
-struct StepPasses {
-  int npass = 0;
-  int pair[kMaxPasses];
-  const void* tab[kMaxPasses];  // (m00, m01, m11) SoA operator table, 3·N entries of cx<T>
-  int refl[kMaxPasses];
+// One pass of a step: operator table ((m00, m01, m11) SoA, 3·N entries of cx<T>, FP32 tables
+// followed by their lo blocks), pair index (into the step's pair-id plane), reflection flag. The
+// records of every step live in device memory (a per-solve pool built once), so a kernel reads
+// pass j as one uniform load instead of indexing a by-value parameter array.
+struct PassRec {
+  const void* tab;
+  int pair;
+  int refl;
 };
 
 template <typename T>
@@ -76,7 +78,7 @@ struct Step2D {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_step2d(Step2D<T> a, StepPasses ps, FftPlan plan, const Tw<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(kPlaneThreads) k_step2d(Step2D<T> a, const PassRec* __restrict__ ps, int npass, FftPlan plan, const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int c = blockIdx.x;
@@ -85,22 +87,22 @@ __global__ void __launch_bounds__(kPlaneThreads) k_step2d(Step2D<T> a, StepPasse
   __syncthreads();
   fft_smem<-1>(buf, plan, tw, 1, tid, nt);
   cx<T>* spec = a.spec;  // interleaved (N, 2), like the field
-  const bool keep_spec = ps.npass > 1 || a.store_spec;
+  const bool keep_spec = npass > 1 || a.store_spec;
   if (keep_spec) {
     for (int q = tid; q < n; q += nt) spec[2 * q + c] = buf[q];
     __syncthreads();
   }
   const long long e = c == 0 ? 0 : 2LL * n;  // m00 for E_x, m11 for E_y
-  for (int j = 0; j < ps.npass; ++j) {
-    const cx<T>* m = static_cast<const cx<T>*>(ps.tab[j]) + e;
+  for (int j = 0; j < npass; ++j) {
+    const cx<T>* m = static_cast<const cx<T>*>(ps[j].tab) + e;
     if (keep_spec)
       for (int q = tid; q < n; q += nt) buf[q] = tmul(spec[2 * q + c], m, q, 3LL * n);
     else
       for (int q = tid; q < n; q += nt) buf[q] = tmul(buf[q], m, q, 3LL * n);
     __syncthreads();
     fft_smem<+1>(buf, plan, tw, 1, tid, nt);
-    const int pair = ps.pair[j];
-    if (!ps.refl[j]) {
+    const int pair = ps[j].pair;
+    if (!ps[j].refl) {
       for (int q = tid; q < n; q += nt)
         if (!a.pid || a.pid[q] == pair) {
           cx<T> v = buf[q] * a.inv_n;
@@ -123,7 +125,9 @@ __global__ void __launch_bounds__(kPlaneThreads) k_step2d(Step2D<T> a, StepPasse
 }
 
 // x transform of `rows` rows × ncomp interleaved components per CTA; smem [x][row][comp].
-template <int DIR, typename T>
+// TOUT: the output is stored transposed, out[(x·ny + y)·ncomp + c] (the layout the column
+// kernel of a slab step reads contiguously); otherwise row-major like the input.
+template <int DIR, typename T, bool TOUT = false>
 __global__ void __launch_bounds__(kPlaneThreads) k_rows_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int rows,
                            FftPlan plan, const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -141,39 +145,50 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_fft(const cx<T>* in, cx<
   }
   __syncthreads();
   fft_smem<DIR>(buf, plan, tw, rows * ncomp, tid, nt);
-  for (int idx = tid; idx < here * per_row; idx += nt) {
-    const int row = idx / per_row, rem = idx - row * per_row;
-    const int x = rem / ncomp, c = rem - x * ncomp;
-    out[(static_cast<long long>(y0 + row) * nx + x) * ncomp + c] = buf[(x * rows + row) * ncomp + c];
+  if constexpr (TOUT) {  // per x a run of `here` rows × ncomp, contiguous in both memories
+    const int run = here * ncomp;
+    for (int idx = tid; idx < nx * run; idx += nt) {
+      const int x = idx / run, rem = idx - x * run;
+      out[(static_cast<long long>(x) * ny + y0) * ncomp + rem] = buf[x * rows * ncomp + rem];
+    }
+  } else {
+    for (int idx = tid; idx < here * per_row; idx += nt) {
+      const int row = idx / per_row, rem = idx - row * per_row;
+      const int x = rem / ncomp, c = rem - x * ncomp;
+      out[(static_cast<long long>(y0 + row) * nx + x) * ncomp + c] = buf[(x * rows + row) * ncomp + c];
+    }
   }
 }
 
 template <typename T>
 struct ColStep {
-  const cx<T>* in;      // x-transformed field (N, 2)
-  cx<T>* work;          // npass planes (N, 2)
-  cx<T>* spec_out;      // full spectrum F{e} (N, 2), or null
+  const cx<T>* in;      // x-transformed field, transposed: in[(x·ny + y)·2 + c]
+  cx<T>* work;          // npass planes, transposed like `in`
+  cx<T>* spec_out;      // full spectrum F{e} (N, 2) row-major, or null
   int ny, nx, cols;
 };
 
 // y transform of a tile of `cols` columns, then per pass: W = M·Ŝ (2×2), inverse y transform,
-// store to work plane j. smem: spectrum tile [y][col][2] and, for several passes, a work tile.
+// store to work plane j. The x-transformed field, the work planes and the operator tables of a
+// 3D solve are stored transposed (x-major), so every column is one contiguous run in memory.
+// smem: spectrum tile [y][col][2] and, for several passes, a work tile.
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, StepPasses ps, FftPlan plan,
+__global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const PassRec* __restrict__ ps, int npass, FftPlan plan,
                             const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* sbuf = reinterpret_cast<cx<T>*>(smem_raw);
   const int ny = a.ny, nx = a.nx, cols = a.cols;
   const long long n = static_cast<long long>(ny) * nx;
   const int tile = ny * cols * 2;
-  cx<T>* wbuf = ps.npass > 1 ? sbuf + tile : sbuf;
+  const int run = 2 * ny;  // one column, both components
+  cx<T>* wbuf = npass > 1 ? sbuf + tile : sbuf;
   const int x0 = blockIdx.x * cols;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int idx = tid; idx < tile; idx += nt) {
-    const int y = idx / (2 * cols), rem = idx - y * 2 * cols;
-    const int xc = rem >> 1, c = rem & 1;
+    const int xc = idx / run, rem = idx - xc * run;
     const int x = x0 + xc;
-    sbuf[idx] = x < nx ? a.in[(static_cast<long long>(y) * nx + x) * 2 + c] : cx<T>{0, 0};
+    sbuf[((rem >> 1) * cols + xc) * 2 + (rem & 1)] =
+        x < nx ? a.in[static_cast<long long>(x) * run + rem] : cx<T>{0, 0};
   }
   __syncthreads();
   fft_smem<-1>(sbuf, plan, tw, 2 * cols, tid, nt);
@@ -183,28 +198,29 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, StepP
       const int x = x0 + (rem >> 1);
       if (x < nx) a.spec_out[(static_cast<long long>(y) * nx + x) * 2 + (rem & 1)] = sbuf[idx];
     }
-  for (int j = 0; j < ps.npass; ++j) {
-    const cx<T>* m = static_cast<const cx<T>*>(ps.tab[j]);
+  for (int j = 0; j < npass; ++j) {
+    const cx<T>* m = static_cast<const cx<T>*>(ps[j].tab);
     for (int idx = tid; idx < ny * cols; idx += nt) {
-      const int y = idx / cols, xc = idx - y * cols;
+      const int xc = idx / ny, y = idx - xc * ny;
       const int x = x0 + xc;
+      const int sidx = y * cols + xc;
       if (x >= nx) {
-        wbuf[2 * idx] = cx<T>{0, 0};
-        wbuf[2 * idx + 1] = cx<T>{0, 0};
+        wbuf[2 * sidx] = cx<T>{0, 0};
+        wbuf[2 * sidx + 1] = cx<T>{0, 0};
         continue;
       }
-      const long long q = static_cast<long long>(y) * nx + x;
-      const cx<T> s0 = sbuf[2 * idx], s1 = sbuf[2 * idx + 1];
-      wbuf[2 * idx] = tmul(s0, m, q, 3 * n) + tmul(s1, m + n, q, 3 * n);
-      wbuf[2 * idx + 1] = tmul(s0, m + n, q, 3 * n) + tmul(s1, m + 2 * n, q, 3 * n);
+      const long long q = static_cast<long long>(x) * ny + y;  // transposed table index
+      const cx<T> s0 = sbuf[2 * sidx], s1 = sbuf[2 * sidx + 1];
+      wbuf[2 * sidx] = tmul(s0, m, q, 3 * n) + tmul(s1, m + n, q, 3 * n);
+      wbuf[2 * sidx + 1] = tmul(s0, m + n, q, 3 * n) + tmul(s1, m + 2 * n, q, 3 * n);
     }
     __syncthreads();
     fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
     cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
     for (int idx = tid; idx < tile; idx += nt) {
-      const int y = idx / (2 * cols), rem = idx - y * 2 * cols;
-      const int x = x0 + (rem >> 1);
-      if (x < nx) w[(static_cast<long long>(y) * nx + x) * 2 + (rem & 1)] = wbuf[idx];
+      const int xc = idx / run, rem = idx - xc * run;
+      const int x = x0 + xc;
+      if (x < nx) w[static_cast<long long>(x) * run + rem] = wbuf[((rem >> 1) * cols + xc) * 2 + (rem & 1)];
     }
     __syncthreads();
   }
@@ -212,7 +228,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, StepP
 
 template <typename T>
 struct RowSelect {
-  const cx<T>* work;        // npass planes (N, 2) after the inverse y transform
+  const cx<T>* work;        // npass planes after the inverse y transform, transposed (x-major)
   cx<T>* out;               // (N, 2)
   const uint8_t* pid;       // or null
   const T* mask;            // or null
@@ -221,14 +237,14 @@ struct RowSelect {
   cx<T>* refl_out;          // (niface, 2) or null
   const cx<T>* add;         // (niface, 2) or null
   cx<T>* xnext;             // or null: also the x transform of the output rows (the next step's
-                            // first transform, fused here)
+                            // first transform, fused here), stored transposed
   int ny, nx, rows;
   T inv_n;
 };
 
 // inverse x transform of each pass for `rows` rows, then select/mask/gather/add.
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, StepPasses ps, FftPlan plan,
+__global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, const PassRec* __restrict__ ps, int npass, FftPlan plan,
                               const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
@@ -239,18 +255,17 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, S
   const int tid = threadIdx.x, nt = blockDim.x;
   const int per_row = nx * 2, total = rows * per_row;
   const int k0 = a.iface ? a.rowoff[y0] : 0, k1 = a.iface ? a.rowoff[y0 + here] : 0;
-  for (int j = 0; j < ps.npass; ++j) {
+  for (int j = 0; j < npass; ++j) {
     const cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
-    for (int idx = tid; idx < total; idx += nt) {
-      const int row = idx / per_row, rem = idx - row * per_row;
-      const int x = rem >> 1, c = rem & 1;
-      buf[(x * rows + row) * 2 + c] =
-          row < here ? w[(static_cast<long long>(y0 + row) * nx + x) * 2 + c] : cx<T>{0, 0};
+    for (int idx = tid; idx < total; idx += nt) {  // per x a run of `rows` rows × 2 (transposed)
+      const int x = idx / (2 * rows), rem = idx - x * 2 * rows;
+      buf[x * rows * 2 + rem] =
+          (rem >> 1) < here ? w[(static_cast<long long>(x) * ny + y0) * 2 + rem] : cx<T>{0, 0};
     }
     __syncthreads();
     fft_smem<+1>(buf, plan, tw, 2 * rows, tid, nt);
-    const int pair = ps.pair[j];
-    if (!ps.refl[j]) {
+    const int pair = ps[j].pair;
+    if (!ps[j].refl) {
       for (int idx = tid; idx < here * per_row; idx += nt) {
         const int row = idx / per_row, rem = idx - row * per_row;
         const int x = rem >> 1, c = rem & 1;
@@ -288,10 +303,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, S
     }
     __syncthreads();
     fft_smem<-1>(buf, plan, tw, 2 * rows, tid, nt);
-    for (int idx = tid; idx < here * per_row; idx += nt) {
-      const int row = idx / per_row, rem = idx - row * per_row;
-      const int x = rem >> 1, c = rem & 1;
-      a.xnext[(static_cast<long long>(y0 + row) * nx + x) * 2 + c] = buf[(x * rows + row) * 2 + c];
+    const int xrun = here * 2;
+    for (int idx = tid; idx < nx * xrun; idx += nt) {
+      const int x = idx / xrun, rem = idx - x * xrun;
+      a.xnext[(static_cast<long long>(x) * ny + y0) * 2 + rem] = buf[x * rows * 2 + rem];
     }
   }
 }
@@ -313,14 +328,18 @@ __global__ void k_convert(cx<To>* dst, const cx<From>* src, long long count) {
   if (i < count) dst[i] = cast<To>(src[i]);
 }
 
+// Operator table of one (kind, ñ_r, ñ_s): entry q is mode (x, y) = (q mod nx, q div nx), or with
+// `transposed` (3D solves, read column by column) (q div ny, q mod ny).
 template <typename T>
 __global__ void k_build_table(cx<T>* out, int kind, cd nr, cd ns, int ny, int nx, double dy,
-                              double dx, double k0, double dz) {
+                              double dx, double k0, double dz, int transposed) {
   const long long n = static_cast<long long>(ny) * nx;
   const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (q >= n) return;
-  const double kx = fftfreq(q % nx, nx, dx);
-  const double ky = fftfreq(q / nx, ny, dy);
+  const long long xi = transposed ? q / ny : q % nx;
+  const long long yi = transposed ? q % ny : q / nx;
+  const double kx = fftfreq(xi, nx, dx);
+  const double ky = fftfreq(yi, ny, dy);
   cd m[3];
   operator_matrix(kind, kx, ky, nr, ns, k0, dz, m);
   for (int e = 0; e < 3; ++e) {

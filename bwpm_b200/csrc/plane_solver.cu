@@ -61,9 +61,10 @@ class PlaneSolver final : public Solver {
   using C = cx<T>;
   void setup();
   // per-step pairs, pair-id planes and interface lists from uint8 labels on the device
-  void device_steps(const std::uint8_t* labels_u8);
+  void device_steps(const std::uint8_t* labels_u8, const std::vector<int>& host_of);
   const C* table(int kind, cd nr, cd ns);
-  StepPasses passes(int step, bool backward, bool reflect);
+  // pass records of all steps on the device (forward, and backward when with_backward)
+  void ensure_passes(bool with_backward);
   // x_ready: xbuf_ already holds the x transform of `in` (3D, fused into the previous step);
   // x_next: also leave the x transform of `out` in xbuf_ for the next step
   void step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out, const C* add,
@@ -81,6 +82,7 @@ class PlaneSolver final : public Solver {
   void add_plane_scaled(C* dst, const C* src, const T* mask);
   LaunchShape rows_shape(int ncomp, int rows_max) const;
   LaunchShape cols_shape(int ncomp, int tiles) const;
+  LaunchShape step_rows_shape() const;
   std::size_t n() const { return in_.ny * in_.nx; }
   bool is2d() const { return in_.nx == 1; }
   cd index_of(int label) const {
@@ -126,6 +128,10 @@ class PlaneSolver final : public Solver {
   int sms_ = 148;
   LaunchShape rows2_, rows3_, sel_, cols1_, cols2_, cols3_;
   std::int64_t launches_ = 0, gmres_applies_ = 0;
+  DevBuf<PassRec> pass_pool_;
+  std::vector<long long> pass_off_[2];
+  std::vector<int> pass_nt_[2], pass_nr_[2];
+  int pool_dirs_ = 0;  // directions in the pool: 0 none, 1 forward, 2 forward and backward
 };
 
 template <typename T>
@@ -139,6 +145,23 @@ LaunchShape PlaneSolver<T>::rows_shape(int ncomp, int rows_max) const {
   s.threads = std::max(64, threads_needed(hx_.plan, s.rows * ncomp));
   if (s.threads > kPlaneThreads) throw invalid_argument("nx too large for the row transform");
   s.smem = s.rows * row_bytes;
+  return s;
+}
+
+// Rows per CTA of the slab-step row kernels (2 components): 4 when that still gives a CTA per
+// SM, else 2, so that every transposed run (rows × 16 B in complex64) fills whole 32-byte sectors.
+template <typename T>
+LaunchShape PlaneSolver<T>::step_rows_shape() const {
+  LaunchShape s;
+  const std::size_t row_bytes = in_.nx * 2 * sizeof(C);
+  int rows = static_cast<int>(in_.ny) / 4 >= sms_ ? 4 : 2;
+  rows = std::min<int>(rows, static_cast<int>(in_.ny));
+  while (rows > 1 && (rows * row_bytes > 98304 || threads_needed(hx_.plan, rows * 2) > kPlaneThreads)) --rows;
+  s.rows = rows;
+  s.threads = std::max(64, threads_needed(hx_.plan, rows * 2));
+  if (s.threads > kPlaneThreads || rows * row_bytes > 227 * 1024)
+    throw invalid_argument("nx too large for the row transform");
+  s.smem = rows * row_bytes;
   return s;
 }
 
@@ -266,12 +289,12 @@ void PlaneSolver<T>::setup() {
         check_cuda(cudaGetLastError(), "k_labels_to_u8");
       }
       lab8 = u8.ptr;
-      device_steps(lab8);
+      device_steps(lab8, host_of);
       int flag = 0;
       check_cuda(cudaMemcpy(&flag, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost), "labels check");
       if (flag) throw invalid_argument("labels must index into `indices`");
     } else {
-      device_steps(lab8);
+      device_steps(lab8, host_of);
     }
     in_.labels_device = nullptr;  // not read after set-up
   } else {
@@ -401,13 +424,14 @@ void PlaneSolver<T>::setup() {
   } else {
     rows2_ = rows_shape(2, 8);
     rows3_ = rows_shape(3, 8);
-    sel_ = rows_shape(2, 8);
+    sel_ = step_rows_shape();
     cols1_ = cols_shape(2, 1);
     cols2_ = cols_shape(2, 2);
     cols3_ = cols_shape(3, 1);
     xbuf_.alloc(2 * nn, stream_);
     work_.alloc(static_cast<std::size_t>(max_pass_) * 2 * nn, stream_);
     for (auto k : {(const void*)k_rows_fft<-1, T>, (const void*)k_rows_fft<1, T>,
+                   (const void*)k_rows_fft<-1, T, true>,
                    (const void*)k_cols_step<T>, (const void*)k_rows_select<T>,
                    (const void*)k_cols_fft<-1, T>, (const void*)k_cols_fft<1, T>})
       check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
@@ -437,7 +461,7 @@ void PlaneSolver<T>::setup() {
 }
 
 template <typename T>
-void PlaneSolver<T>::device_steps(const std::uint8_t* labels_u8) {
+void PlaneSolver<T>::device_steps(const std::uint8_t* labels_u8, const std::vector<int>& host_of) {
   const std::size_t nn = n();
   const int nz = static_cast<int>(in_.nz);
   const int m = static_cast<int>(in_.indices.size());
@@ -507,6 +531,7 @@ void PlaneSolver<T>::device_steps(const std::uint8_t* labels_u8) {
         rowoff_off.push_back(-1);
       }
     }
+    st.host_slot = host_of[p];  // Born slab (δn) or −1
     int npass = static_cast<int>(st.pairs.size());
     for (auto& pr : st.pairs) {
       const cd x = index_of(pr.first), y = index_of(pr.second);
@@ -553,42 +578,59 @@ const cx<T>* PlaneSolver<T>::table(int kind, cd nr, cd ns) {
   if (it != tables_.end()) return it->second.ptr;
   DevBuf<C> t(table_blocks<T>() * n(), stream_);
   launch(k_build_table<T>, dim3(ceil_div(n(), kThreads)), dim3(kThreads), 0, t.ptr, kind, nr, ns,
-         static_cast<int>(in_.ny), static_cast<int>(in_.nx), in_.dy, in_.dx, in_.k0, in_.dz);
+         static_cast<int>(in_.ny), static_cast<int>(in_.nx), in_.dy, in_.dx, in_.k0, in_.dz,
+         is2d() ? 0 : 1);
   const C* ptr = t.ptr;
   tables_.emplace(key, std::move(t));
   return ptr;
 }
 
+// Pass records of every step in one device pool, built before the first run that needs them:
+// per step and direction the transmissions (all pairs), then the reflections (pairs whose
+// indices differ); a step without reflection uses the first part only. Forward step s:
+// (r, s) = (plane s, plane s + 1); the backward step from plane s + 1 to plane s swaps the
+// roles (cpp/src/solver_cuda.cu:615-624).
 template <typename T>
-StepPasses PlaneSolver<T>::passes(int s, bool backward, bool reflect) {
-  // forward step s: (r, s) = (plane s, plane s + 1); backward step from plane s + 1 to plane s
-  // swaps the roles (cpp/src/solver_cuda.cu:615-624)
-  const StepInfo& st = steps_[s];
-  StepPasses ps;
-  ps.npass = 0;
-  for (int pass = 0; pass < 2; ++pass) {
-    if (pass == 1 && !reflect) break;
-    for (std::size_t i = 0; i < st.pairs.size(); ++i) {
-      const int lr = backward ? st.pairs[i].second : st.pairs[i].first;
-      const int ls = backward ? st.pairs[i].first : st.pairs[i].second;
-      const cd nr = index_of(lr), ns = index_of(ls);
-      const bool same = nr.re == ns.re && nr.im == ns.im;
-      if (pass == 1 && same) continue;
-      const int kind = pass == 0 ? (backward ? kBwdT : kFwdT) : (backward ? kBwdR : kFwdR);
-      ps.pair[ps.npass] = static_cast<int>(i);
-      ps.tab[ps.npass] = table(kind, nr, ns);
-      ps.refl[ps.npass] = pass;
-      ++ps.npass;
+void PlaneSolver<T>::ensure_passes(bool with_backward) {
+  if (pool_dirs_ >= (with_backward ? 2 : 1)) return;
+  const int dirs = with_backward ? 2 : 1;
+  std::vector<PassRec> host;
+  for (int d = 0; d < 2; ++d) {
+    pass_off_[d].assign(in_.nz, 0);
+    pass_nt_[d].assign(in_.nz, 0);
+    pass_nr_[d].assign(in_.nz, 0);
+  }
+  for (int d = 0; d < dirs; ++d) {
+    const bool backward = d == 1;
+    for (std::size_t s = 0; s < in_.nz; ++s) {
+      const StepInfo& st = steps_[s];
+      pass_off_[d][s] = static_cast<long long>(host.size());
+      for (int pass = 0; pass < 2; ++pass) {
+        for (std::size_t i = 0; i < st.pairs.size(); ++i) {
+          const int lr = backward ? st.pairs[i].second : st.pairs[i].first;
+          const int ls = backward ? st.pairs[i].first : st.pairs[i].second;
+          const cd nr = index_of(lr), ns = index_of(ls);
+          const bool same = nr.re == ns.re && nr.im == ns.im;
+          if (pass == 1 && same) continue;
+          const int kind = pass == 0 ? (backward ? kBwdT : kFwdT) : (backward ? kBwdR : kFwdR);
+          host.push_back(PassRec{table(kind, nr, ns), static_cast<int>(i), pass});
+          ++(pass == 0 ? pass_nt_[d][s] : pass_nr_[d][s]);
+        }
+      }
     }
   }
-  return ps;
+  pass_pool_.alloc(host.size(), stream_);
+  pass_pool_.upload(host.data(), host.size());
+  pool_dirs_ = dirs;
 }
 
 template <typename T>
 void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out,
                           const C* add, bool want_spec, bool x_ready, bool x_next) {
   const StepInfo& st = steps_[s];
-  const StepPasses ps = passes(s, backward, reflect);
+  const int dir = backward ? 1 : 0;
+  const PassRec* ps = pass_pool_.ptr + pass_off_[dir][s];
+  const int npass = pass_nt_[dir][s] + (reflect ? pass_nr_[dir][s] : 0);
   const std::uint8_t* pid = st.pid_off >= 0 ? pid_pool_.ptr + st.pid_off : nullptr;
   const int* iface = st.niface > 0 ? iface_pool_.ptr + st.iface_off : nullptr;
   // FP32 tables carry the inverse transform's 1/N already
@@ -607,16 +649,16 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
     a.n = static_cast<int>(n());
     a.store_spec = want_spec ? 1 : 0;
     a.inv_n = inv_n;
-    launch(k_step2d<T>, dim3(2), dim3(thr2d_), n() * sizeof(C), a, ps, hy_.plan, tw_y_.ptr);
+    launch(k_step2d<T>, dim3(2), dim3(thr2d_), n() * sizeof(C), a, ps, npass, hy_.plan, tw_y_.ptr);
     return;
   }
   const int ny = static_cast<int>(in_.ny), nx = static_cast<int>(in_.nx);
-  if (!x_ready)
-    launch(k_rows_fft<-1, T>, dim3(ceil_div(ny, rows2_.rows)), dim3(rows2_.threads), rows2_.smem, in,
-           xbuf_.ptr, ny, nx, 2, rows2_.rows, hx_.plan, tw_x_.ptr);
-  const LaunchShape& cs = ps.npass > 1 ? cols2_ : cols1_;
+  if (!x_ready)  // the x transform of the step's input, stored transposed for the column kernel
+    launch(k_rows_fft<-1, T, true>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, in,
+           xbuf_.ptr, ny, nx, 2, sel_.rows, hx_.plan, tw_x_.ptr);
+  const LaunchShape& cs = npass > 1 ? cols2_ : cols1_;
   ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cs.rows};
-  launch(k_cols_step<T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem, c, ps, hy_.plan,
+  launch(k_cols_step<T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem, c, ps, npass, hy_.plan,
          tw_y_.ptr);
   RowSelect<T> r;
   r.work = work_.ptr;
@@ -632,7 +674,7 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   r.nx = nx;
   r.rows = sel_.rows;
   r.inv_n = inv_n;
-  launch(k_rows_select<T>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, r, ps,
+  launch(k_rows_select<T>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, r, ps, npass,
          hx_.plan, tw_x_.ptr);
 }
 
@@ -910,6 +952,7 @@ void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* ke
     t_iter.alloc(iterations * 2 * nn, stream_);
     r_iter.alloc(iterations * 2 * nn, stream_);
   }
+  ensure_passes(iterations > 0);
   check_cuda(cudaMemcpyAsync(stage_.ptr, field, n2 * sizeof(cd), cudaMemcpyHostToDevice, stream_), "field upload");
   launch(k_convert<T, double>, dim3(ceil_div(n2, kThreads)), dim3(kThreads), 0, input_.ptr,
          (const cd*)stage_.ptr, n2);

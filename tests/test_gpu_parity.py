@@ -198,17 +198,19 @@ def test_run_twice_is_deterministic(core):
     assert np.array_equal(r1["reflected"], r2["reflected"])
 
 
-@pytest.mark.parametrize("prefix,iters", [("volume1.", 2), ("volume2.", 2), ("volume3.", 2)])
+@pytest.mark.parametrize("prefix,iters", [("volume1.", 2), ("volume2.", 2), ("volume3.", 2),
+                                          ("fluct1.", 1), ("backscatter.", 3)])
 @pytest.mark.parametrize("precision", [64, 32])
 def test_device_setup_equals_host_setup(core, monkeypatch, prefix, iters, precision):
     """The per-step tables built on the device (plane_setup.cuh) give bit-identical results to
-    the host set-up, FP64 and complex64, with keep planes and stored sources."""
+    the host set-up, FP64 and complex64, with keep planes, stored sources and Born slabs."""
     d = load_npz("random_volumes.npz")
-    args, field, _ = volume_case(d, prefix)
+    args, field, fl = volume_case(d, prefix)
     out = {}
     for where in ("host", "device"):
         monkeypatch.setenv("BWPM_SETUP", where)
-        out[where] = core.CudaSolver(*args, 0, precision=precision).run(field, iters, [0, 5])
+        out[where] = core.CudaSolver(*args, 0, fluctuation=fl, precision=precision).run(
+            field, iters, [0, 5])
     a, b = out["host"], out["device"]
     for key in ("transmitted", "reflected"):
         assert np.array_equal(a[key], b[key]), key
