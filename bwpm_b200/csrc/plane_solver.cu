@@ -70,7 +70,8 @@ class PlaneSolver final : public Solver {
   void step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out, const C* add,
             bool want_spec, bool x_ready = false, bool x_next = false);
   void fft_plane(const C* in, C* out, int ncomp, int dir);
-  void born_operator(const C* in, C* out, int slot, int dir);
+  // out = G·in (combine 0) or in − G·in/2 (combine 1)
+  void born_operator(const C* in, C* out, int slot, int dir, int combine = 0);
   void born_step(const C* spec, C* inc, int slot, int dir);
   void born_sources(const C* spec, int slot, int dir);
   void born_emission(int slot, int dir, C* plane);
@@ -117,7 +118,8 @@ class PlaneSolver final : public Solver {
   // Born
   std::vector<cd> hosts_;
   DevBuf<C> pot_, born_fwd_, born_bwd_, w3_, t3_, sources_, g_x_, g_rhs_, g_y_, g_w_, g_tmp_,
-      inc_;
+      g_tmp2_, inc_;
+  bool born2d_fused_ = false;  // 2D Born operator in one kernel (three lines fit shared memory)
   std::vector<DevBuf<C>> basis_;
   DevBuf<GmresState> gst_;
   DevBuf<cd> dot_partial_;
@@ -455,7 +457,11 @@ void PlaneSolver<T>::setup() {
     w3_.alloc(3 * nn, stream_);
     t3_.alloc(3 * nn, stream_);
     sources_.alloc(6 * nn, stream_);
-    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &inc_}) b->alloc(2 * nn, stream_);
+    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &g_tmp2_, &inc_}) b->alloc(2 * nn, stream_);
+    born2d_fused_ = is2d() && 3 * nn * sizeof(C) <= 227 * 1024;
+    if (born2d_fused_)
+      check_cuda(cudaFuncSetAttribute(k_born_op2d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      227 * 1024), "smem");
   }
   check_cuda(cudaStreamSynchronize(stream_), "setup");  // this solver's stream only
 }
@@ -707,10 +713,15 @@ void PlaneSolver<T>::fft_plane(const C* in, C* out, int ncomp, int dir) {
 }
 
 template <typename T>
-void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir) {
+void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir, int combine) {
   // cpp/src/solver.cpp:262-311
   const BornGrid g = born_grid(slot);
   const long long nn = static_cast<long long>(n());
+  if (born2d_fused_) {  // 2D: one kernel (k_born_op2d)
+    launch(k_born_op2d<T>, dim3(1), dim3(thr_line3_), 3 * n() * sizeof(C), in, out,
+           (const C*)(pot_.ptr + slot * nn), g, dir, combine, hy_.plan, tw_y_.ptr);
+    return;
+  }
   launch(k_born_prepare<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, in, w3_.ptr, g, dir, 0.0);
   fft_plane(w3_.ptr, w3_.ptr, 3, +1);
   launch(k_born_potential<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr,
@@ -718,6 +729,11 @@ void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir) {
   fft_plane(w3_.ptr, w3_.ptr, 3, -1);
   launch(k_born_finish<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, (const C*)w3_.ptr, out,
          g, dir);
+  if (combine) {  // out = in − G·in/2
+    check_cuda(cudaMemcpyAsync(g_tmp2_.ptr, out, 2 * nn * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(out, in, 2 * nn * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+    axpby(out, g_tmp2_.ptr, cd{-0.5, 0.0}, cd{1.0, 0.0}, 2 * nn);
+  }
 }
 
 template <typename T>
@@ -757,10 +773,8 @@ void PlaneSolver<T>::gmres(int slot, int dir) {
     launch(k_dot_dev<T>, dim3(dblocks), dim3(256), 0, u, v, m2, dot_partial_.ptr, &st->counter, out);
   };
   auto apply = [&](const C* v, C* av) {  // av = v − G v/2
-    born_operator(v, g_tmp_.ptr, slot, dir);
+    born_operator(v, av, slot, dir, 1);
     ++gmres_applies_;
-    check_cuda(cudaMemcpyAsync(av, v, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
-    axpby(av, g_tmp_.ptr, cd{-0.5, 0.0}, cd{1.0, 0.0}, m2);
   };
   auto host_norm = [&](const C* u) {  // ‖u‖ read back on the host
     dot_into(u, u, &st->dot);
