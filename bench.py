@@ -447,8 +447,39 @@ def run_ours(args) -> None:
         "setup_s": setup_s,
         "device_bytes": stats["device_bytes"],
     }
+    # the figures a reader of the line's tail needs, last
+    line["summary"] = _summary(line)
     print(json.dumps(line), flush=True)
     _barrier(dist)
+
+
+def _summary(line: dict) -> dict:
+    """A compact digest of the line (parity, the FP64 and CPU comparisons, served, configs)."""
+    def get(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict):
+                return None
+            d = d.get(k)
+        return d
+
+    cfg = line.get("configs") or {}
+    return {
+        "solves_per_s": line["value"], "e2e_solves_per_s": get(line, "e2e", "value"),
+        "l2_err_max_vs_fp64": line.get("l2_err_max"), "eps_err_max_vs_fp64": line.get("eps_err_max"),
+        "speedup_vs_fp64_plain": get(line, "fp64_plain", "speedup_batched_c64"),
+        "speedup_vs_reference_cuda_fp64": get(line, "fp64_plain", "reference_cuda_core",
+                                              "speedup_batched_c64"),
+        "cpu_reference_solves_per_s": get(line, "cpu_baseline", "value"),
+        "fp32_frac": get(line, "roofline", "frac"),
+        "served_solves_per_s": get(line, "served", "solves_per_s"),
+        "served_p50_p99_ms": [get(line, "served", "p50_ms"), get(line, "served", "p99_ms")],
+        "served_speedup_vs_fp64": get(line, "served", "speedup_vs_fp64_plain"),
+        "cfg1_ms_c64_both_fp64_each": [get(cfg, "slab2d", "c64_batched_ms_both"),
+                                       get(cfg, "slab2d", "fp64_ms_per_solve")],
+        "cfg2_s_c64_fp64": [get(cfg, "born2d", "c64_s"), get(cfg, "born2d", "fp64_s")],
+        "cfg3_s_c64_fp64_refcuda": [get(cfg, "microlens3d", "c64_s"), get(cfg, "microlens3d", "fp64_s"),
+                                    get(cfg, "microlens3d", "reference_cuda_fp64_s")],
+    }
 
 
 # ---- served request stream (continuous batching) ----------------------------------------------
@@ -571,9 +602,10 @@ def _reference_cuda_core():
 
 
 def run_configs(device: int) -> dict:
-    """Configurations 1-3 on this GPU: complex64 result of this implementation against the
-    per-solve FP64 drop-in path (time and relative L2 error), and for the 2D slab the reference's
-    CPU core on one thread. Born (configuration 2) runs on a reduced chain, stated in the entry."""
+    """Configurations 1-3 on this GPU: the complex64 result of this implementation against the
+    per-solve FP64 drop-in path (time and relative L2 error), the reference's own GPU core
+    (cuFFT, FP64; staged build) on the same solves, and for the 2D slab the reference's CPU core
+    on one thread. Configuration 2 (Born) runs at full size in TE; times include set-up."""
     from bwpm_b200 import _core, workloads
     from bwpm_b200.batch import Batch2D
 
@@ -582,6 +614,8 @@ def run_configs(device: int) -> dict:
         r = fn()
         return r, time.perf_counter() - t0
 
+    ref_core = _reference_core()
+    ref_cuda = _reference_cuda_core()
     out: dict = {}
     # 1: 5 um slab, 1024 points, 250 slabs, 8 iterations, TE and TM
     probs = [workloads.slab2d("te"), workloads.slab2d("tm")]
@@ -590,8 +624,7 @@ def run_configs(device: int) -> dict:
     b.prepare()
     b.run()
     batch_ms = b.run()
-    ref_core = _reference_core()
-    t64, tcpu, errs = [], [], []
+    t64, tcpu, tref, errs = [], [], [], []
     for p, i in zip(probs, ids):
         r64, dt = timed(lambda p=p: _core.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))
         t64.append(dt)
@@ -601,40 +634,61 @@ def run_configs(device: int) -> dict:
         if ref_core is not None:
             _, dt = timed(lambda p=p: ref_core.Solver(*p.core_args(), 1).run(p.field, p.iterations, []))
             tcpu.append(dt)
+        if ref_cuda is not None:
+            _, dt = timed(lambda p=p: ref_cuda.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))
+            tref.append(dt)
     out["slab2d"] = {"solves": 2, "c64_batched_ms_both": batch_ms,
                      "fp64_ms_per_solve": 1e3 * float(np.mean(t64)),
+                     "reference_cuda_fp64_ms_per_solve": 1e3 * float(np.mean(tref)) if tref else None,
                      "cpu_reference_ms_per_solve": 1e3 * float(np.mean(tcpu)) if tcpu else None,
                      "cpu_threads": 1, "l2_err_max": float(np.max(errs)),
                      "workload": "1024 points, 250 slabs of lambda/10, 5 um slab n=1.5 in air, "
                                  "8 iterations, TE and TM"}
+    del b
     # 3: microlens with a tilted silver back face, 512^2 points, 400 slabs, 6 iterations
     p = workloads.microlens3d()
-    r32, t32 = timed(lambda: _core.CudaSolver(*p.core_args(), device, precision=32).run(p.field, p.iterations, []))
-    r64, t64s = timed(lambda: _core.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))
+    points_passes = p.ny * p.nx * p.nz * 2 * p.iterations
+    s32, t32_setup = timed(lambda: _core.CudaSolver(*p.core_args(), device, precision=32))
+    r32, t32 = timed(lambda: s32.run(p.field, p.iterations, []))
+    del s32
+    s64, t64_setup = timed(lambda: _core.CudaSolver(*p.core_args(), device))
+    r64, t64s = timed(lambda: s64.run(p.field, p.iterations, []))
+    del s64
+    tref3 = None
+    if ref_cuda is not None:
+        _, tref3 = timed(lambda: ref_cuda.CudaSolver(*p.core_args(), device).run(p.field, p.iterations, []))
     # the silver fills everything behind the back face: the transmitted field is ~1e-94 of the
     # incident one in FP64, below the complex64 range, so errors are relative to the larger of
     # the field's own norm and 1e-6 of the incident field's
     floor = 1e-6 * float(np.linalg.norm(p.field))
-    out["microlens3d"] = {"c64_s": t32, "fp64_s": t64s,
+    out["microlens3d"] = {"c64_s": t32_setup + t32, "c64_run_s": t32, "fp64_s": t64_setup + t64s,
+                          "fp64_run_s": t64s,
+                          "reference_cuda_fp64_s": tref3,
                           "l2_err": max(_rel_floor(r32["transmitted"], r64["transmitted"], floor),
                                         _rel_floor(r32["reflected"], r64["reflected"], floor)),
                           "l2_err_reflected": _rel(r32["reflected"], r64["reflected"]),
                           "transmitted_norm_over_incident": float(np.linalg.norm(r64["transmitted"])) /
                                                             float(np.linalg.norm(p.field)),
                           "workload": "512^2 points, 400 slabs of lambda/8, lens n=1.52 + silver, "
-                                      "6 iterations; set-up (labels -> step records) included"}
+                                      "6 iterations; *_s include set-up (labels -> step tables)"}
+    # seconds per grid point and pass (one direction of one iteration): the runtime model of
+    # the reference's adapter (src/bwpm/adapter.py:35), measured on this configuration
+    out["seconds_per_point_pass"] = {"cuda_fp64": t64s / points_passes, "cuda_c64": t32 / points_passes,
+                                     "reference_cuda_fp64": tref3 / points_passes if tref3 else None,
+                                     "reference_value_cuda": 4.6e-8,
+                                     "workload": "microlens 512^2 x 400 slabs x 6 iterations, run only"}
     del r32, r64, p
-    # 2 (reduced chain): Born fluctuation, 4096 points, 100 of the 2000 slabs, 1 of 6 iterations
-    p = workloads.born2d(nz=100, iterations=1)
+    # 2: Born fluctuation at full size, 4096 points, 2000 slabs, 6 iterations, TE
+    p = workloads.born2d(polarization="te")
     r32, t32 = timed(lambda: _core.CudaSolver(*p.core_args(), device, fluctuation=p.fluctuation,
                                               precision=32).run(p.field, p.iterations, []))
     r64, t64s = timed(lambda: _core.CudaSolver(*p.core_args(), device,
                                                fluctuation=p.fluctuation).run(p.field, p.iterations, []))
-    out["born2d_reduced"] = {"c64_s": t32, "fp64_s": t64s,
-                             "l2_err": max(_rel(r32["transmitted"], r64["transmitted"]),
-                                           _rel(r32["reflected"], r64["reflected"])),
-                             "workload": "4096 points, 100 of 2000 slabs, 1 of 6 iterations, "
-                                         "delta-n on every slab; set-up included"}
+    out["born2d"] = {"c64_s": t32, "fp64_s": t64s,
+                     "l2_err_transmitted": _rel(r32["transmitted"], r64["transmitted"]),
+                     "l2_err_reflected": _rel(r32["reflected"], r64["reflected"]),
+                     "workload": "4096 points, 2000 slabs, delta-n (std 0.01, 0.5 um) on every slab, "
+                                 "10 deg plane wave, 6 iterations, TE; set-up included"}
     return out
 
 

@@ -35,6 +35,17 @@ __device__ __forceinline__ cx<T> tmul(cx<T> u, const cx<T>* m, long long q, long
   }
 }
 
+// Table entry e (0: m00, 1: m01, 2: m11) from a point's loaded table values (kB of them: FP64
+// one value per entry; FP32 hi values then lo values), times a field value; as tmul.
+template <typename T, int KB>
+__device__ __forceinline__ cx<T> tmul_v(cx<T> u, const cx<T> (&tv)[KB], int e) {
+  if constexpr (sizeof(T) == sizeof(double)) {
+    return u * tv[e];
+  } else {
+    return pmul(u, tv[e], tv[3 + e]);
+  }
+}
+
 // Field value times the mask (FP32 masks hold hi values then lo values, `n` apart).
 template <typename T>
 __device__ __forceinline__ cx<T> mmul(cx<T> v, const T* mask, long long q, long long n) {
@@ -198,21 +209,39 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
       const int x = x0 + (rem >> 1);
       if (x < nx) a.spec_out[(static_cast<long long>(y) * nx + x) * 2 + (rem & 1)] = sbuf[idx];
     }
+  constexpr int kB = table_blocks<T>();  // table values per point (3 entries, FP32: + lo parts)
+  constexpr int U = 4;                   // points per thread whose table values load together
   for (int j = 0; j < npass; ++j) {
     const cx<T>* m = static_cast<const cx<T>*>(ps[j].tab);
-    for (int idx = tid; idx < ny * cols; idx += nt) {
-      const int xc = idx / ny, y = idx - xc * ny;
-      const int x = x0 + xc;
-      const int sidx = y * cols + xc;
-      if (x >= nx) {
-        wbuf[2 * sidx] = cx<T>{0, 0};
-        wbuf[2 * sidx + 1] = cx<T>{0, 0};
-        continue;
+    for (int base = tid; base < ny * cols; base += U * nt) {
+      cx<T> tv[U][kB];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {  // every table value of U points in flight at once
+        const int idx = base + u * nt;
+        const int xc = idx / ny, y = idx - xc * ny;
+        const int x = x0 + xc;
+        if (idx < ny * cols && x < nx) {
+          const long long q = static_cast<long long>(x) * ny + y;  // transposed table index
+#pragma unroll
+          for (int b = 0; b < kB; ++b) tv[u][b] = m[b * n + q];
+        }
       }
-      const long long q = static_cast<long long>(x) * ny + y;  // transposed table index
-      const cx<T> s0 = sbuf[2 * sidx], s1 = sbuf[2 * sidx + 1];
-      wbuf[2 * sidx] = tmul(s0, m, q, 3 * n) + tmul(s1, m + n, q, 3 * n);
-      wbuf[2 * sidx + 1] = tmul(s0, m + n, q, 3 * n) + tmul(s1, m + 2 * n, q, 3 * n);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + u * nt;
+        if (idx >= ny * cols) break;
+        const int xc = idx / ny, y = idx - xc * ny;
+        const int x = x0 + xc;
+        const int sidx = y * cols + xc;
+        if (x >= nx) {
+          wbuf[2 * sidx] = cx<T>{0, 0};
+          wbuf[2 * sidx + 1] = cx<T>{0, 0};
+          continue;
+        }
+        const cx<T> s0 = sbuf[2 * sidx], s1 = sbuf[2 * sidx + 1];
+        wbuf[2 * sidx] = tmul_v(s0, tv[u], 0) + tmul_v(s1, tv[u], 1);
+        wbuf[2 * sidx + 1] = tmul_v(s0, tv[u], 1) + tmul_v(s1, tv[u], 2);
+      }
     }
     __syncthreads();
     fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);

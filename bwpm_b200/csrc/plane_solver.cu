@@ -160,7 +160,7 @@ LaunchShape PlaneSolver<T>::step_rows_shape() const {
   rows = std::min<int>(rows, static_cast<int>(in_.ny));
   while (rows > 1 && (rows * row_bytes > 98304 || threads_needed(hx_.plan, rows * 2) > kPlaneThreads)) --rows;
   s.rows = rows;
-  s.threads = std::max(64, threads_needed(hx_.plan, rows * 2));
+  s.threads = std::max(256, threads_needed(hx_.plan, rows * 2));
   if (s.threads > kPlaneThreads || rows * row_bytes > 227 * 1024)
     throw invalid_argument("nx too large for the row transform");
   s.smem = rows * row_bytes;
@@ -177,7 +177,9 @@ LaunchShape PlaneSolver<T>::cols_shape(int ncomp, int tiles) const {
                       threads_needed(hy_.plan, cols * ncomp) > kPlaneThreads))
     --cols;
   s.rows = cols;
-  s.threads = std::max(64, threads_needed(hy_.plan, cols * ncomp));
+  // at least 256 threads: a column's loads and stores are spread over more warps than its
+  // transform needs (the kernels are latency-bound otherwise: one column per CTA at 512²)
+  s.threads = std::min(kPlaneThreads, std::max(256, threads_needed(hy_.plan, cols * ncomp)));
   s.smem = col_bytes * cols * tiles;
   if (s.threads > kPlaneThreads || s.smem > 227 * 1024)
     throw invalid_argument("ny too large for the column transform");
