@@ -142,64 +142,6 @@ __global__ void k_axpby(cx<T>* y, const cx<T>* x, cd a, cd b, long long m) {
   y[i] = cast<T>(a * cast<double>(x[i]) + b * cast<double>(y[i]));
 }
 
-// ---- the Born operator of a 2D slab in one kernel ------------------------------------------
-
-// out = G_d·in (combine = 0) or out = in − G_d·in/2 (combine = 1, the GMRES operator of the Cayley
-// step) for a 2D plane (nx = 1) in one CTA: prepare, the three inverse line transforms, the
-// potential, the three forward transforms and the finish of k_born_prepare / fft_plane /
-// k_born_potential / k_born_finish (and k_axpby), with the same arithmetic in the same order and
-// the three component lines in shared memory (3·ny values) instead of five launches and an
-// (N, 3) plane round trip each.
-template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads)
-    k_born_op2d(const cx<T>* in, cx<T>* out, const cx<T>* pot, BornGrid g, int direction,
-                int combine, FftPlan plan, const Tw<T>* __restrict__ tw) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);  // three lines of ny values
-  const int n = g.ny, tid = threadIdx.x, nt = blockDim.x;
-  for (int q = tid; q < n; q += nt) {
-    const BornPoint p = born_point(g, q);
-    if (!p.prop) {
-      buf[q] = buf[n + q] = buf[2 * n + q] = cx<T>{0, 0};
-      continue;
-    }
-    const cd ex = cast<double>(in[2 * q]), ey = cast<double>(in[2 * q + 1]);
-    const cd ez = cdiv(-static_cast<double>(direction) * (p.kx * ex + p.ky * ey), p.kz);
-    const cd ph{1.0, 0.0};
-    buf[q] = cast<T>(ex * ph);
-    buf[n + q] = cast<T>(ey * ph);
-    buf[2 * n + q] = cast<T>(ez * ph);
-  }
-  __syncthreads();
-  for (int c = 0; c < 3; ++c) fft_smem<+1>(buf + c * n, plan, tw, 1, tid, nt);
-  const T inv_n = static_cast<T>(1.0 / static_cast<double>(n));
-  for (int q = tid; q < n; q += nt) {
-    const cx<T> s = pot[q] * inv_n;
-    for (int c = 0; c < 3; ++c) buf[c * n + q] = s * buf[c * n + q];
-  }
-  __syncthreads();
-  for (int c = 0; c < 3; ++c) fft_smem<-1>(buf + c * n, plan, tw, 1, tid, nt);
-  const cd k = g.host * g.k0;
-  const cd k2 = k * k;
-  for (int q = tid; q < n; q += nt) {
-    const BornPoint p = born_point(g, q);
-    cx<T> o0{0, 0}, o1{0, 0};
-    if (p.prop) {
-      const cd green = cdiv(cd{0.0, g.dz}, 2.0 * p.kz);
-      const cd s0 = cast<double>(buf[q]), s1 = cast<double>(buf[n + q]), s2 = cast<double>(buf[2 * n + q]);
-      const cd lon = cdiv(p.kx * s0 + p.ky * s1 + (static_cast<double>(direction) * p.kz) * s2, k2);
-      o0 = cast<T>(green * (s0 - p.kx * lon));
-      o1 = cast<T>(green * (s1 - p.ky * lon));
-    }
-    if (combine) {  // v − G v/2 as k_axpby(av = v, G v, −½, 1)
-      o0 = cast<T>(cd{-0.5, 0.0} * cast<double>(o0) + cd{1.0, 0.0} * cast<double>(in[2 * q]));
-      o1 = cast<T>(cd{-0.5, 0.0} * cast<double>(o1) + cd{1.0, 0.0} * cast<double>(in[2 * q + 1]));
-    }
-    out[2 * q] = o0;
-    out[2 * q + 1] = o1;
-  }
-}
-
 // ---- transforms of planes with ncomp interleaved components ---------------------------------
 
 // nx = 1: one CTA per component, the whole line in shared memory.

@@ -119,7 +119,6 @@ class PlaneSolver final : public Solver {
   std::vector<cd> hosts_;
   DevBuf<C> pot_, born_fwd_, born_bwd_, w3_, t3_, sources_, g_x_, g_rhs_, g_y_, g_w_, g_tmp_,
       g_tmp2_, inc_;
-  bool born2d_fused_ = false;  // 2D Born operator in one kernel (three lines fit shared memory)
   std::vector<DevBuf<C>> basis_;
   DevBuf<GmresState> gst_;
   DevBuf<cd> dot_partial_;
@@ -460,10 +459,6 @@ void PlaneSolver<T>::setup() {
     t3_.alloc(3 * nn, stream_);
     sources_.alloc(6 * nn, stream_);
     for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &g_tmp2_, &inc_}) b->alloc(2 * nn, stream_);
-    born2d_fused_ = is2d() && 3 * nn * sizeof(C) <= 227 * 1024;
-    if (born2d_fused_)
-      check_cuda(cudaFuncSetAttribute(k_born_op2d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      227 * 1024), "smem");
   }
   check_cuda(cudaStreamSynchronize(stream_), "setup");  // this solver's stream only
 }
@@ -719,11 +714,6 @@ void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir, int c
   // cpp/src/solver.cpp:262-311
   const BornGrid g = born_grid(slot);
   const long long nn = static_cast<long long>(n());
-  if (born2d_fused_) {  // 2D: one kernel (k_born_op2d)
-    launch(k_born_op2d<T>, dim3(1), dim3(thr_line3_), 3 * n() * sizeof(C), in, out,
-           (const C*)(pot_.ptr + slot * nn), g, dir, combine, hy_.plan, tw_y_.ptr);
-    return;
-  }
   launch(k_born_prepare<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, in, w3_.ptr, g, dir, 0.0);
   fft_plane(w3_.ptr, w3_.ptr, 3, +1);
   launch(k_born_potential<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr,

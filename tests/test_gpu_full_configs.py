@@ -7,7 +7,8 @@ compiled CPU core (cpp/src/solver.cpp:444-528) on
 - microlens3d: 512² points, 400 slabs, spherical-cap lens n = 1.52 with a 5°-tilted silver back
   face, mask, 6 iterations (bwpm_b200.workloads.microlens3d), stored as the fields at a seeded
   subset of 16384 pixels plus 8 seeded complex projections of each whole field.
-FP64 at relative L2 ≤ 1e-10; complex64 at ≤ 1e-4. Behind the silver the transmitted field is
+FP64 at relative L2 ≤ 1e-10; complex64 at ≤ 1e-4 (the Born reflected field: 1e-3, see
+C64_TOL_BORN_REFLECTED). Behind the silver the transmitted field is
 ≈ 1e-94 of the incident one, below the complex64 range (its smallest normal is ≈ 1e-38), so the
 complex64 transmitted field of configuration 3 is checked against a floor of 1e-6 of the
 incident field's norm: ‖E − E_ref‖ ≤ 1e-4 · max(‖E_ref‖, 1e-6 ‖E_in‖).
@@ -23,6 +24,11 @@ from conftest import load_npz, rel_l2
 pytestmark = pytest.mark.gpu
 
 FP64_TOL, C64_TOL = 1e-10, 1e-4
+# The reflected field of the Born configuration is pure back-scatter, and the reference's own
+# iteration diverges on it (its norm grows 1.3 → 102 over the 6 iterations in TE, 0.40 → 8.4 in
+# TM, ≈ 2.5× per iteration), so rounding differences grow with it: complex64 lands at 8e-5 (TE)
+# and 3.2e-4 (TM) of it, independent of the GMRES tolerance (1e-6 … 3e-8 measured). Held to 1e-3.
+C64_TOL_BORN_REFLECTED = 1e-3
 
 
 @pytest.fixture(scope="module")
@@ -49,8 +55,9 @@ def test_born2d_full_size(full, pol, precision):
     p = workloads.born2d(polarization=pol)
     r = _core.CudaSolver(*p.core_args(), 0, fluctuation=p.fluctuation,
                          precision=precision).run(p.field, p.iterations, [])
-    tol = FP64_TOL if precision == 64 else C64_TOL
     for key in ("transmitted", "reflected"):
+        tol = FP64_TOL if precision == 64 else (C64_TOL_BORN_REFLECTED if key == "reflected"
+                                                else C64_TOL)
         ref = full[f"born2d_{pol}.{key}"]
         assert rel_l2(r[key], ref) < tol, (key, rel_l2(r[key], ref))
         norms = np.array([np.linalg.norm(x) for x in r[f"{key}_iter"]])
