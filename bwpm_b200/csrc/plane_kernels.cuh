@@ -66,10 +66,14 @@ constexpr int table_blocks() {
 // followed by their lo blocks), pair index (into the step's pair-id plane), reflection flag. The
 // records of every step live in device memory (a per-solve pool built once), so a kernel reads
 // pass j as one uniform load instead of indexing a by-value parameter array.
+// `scalar`: a complex64 transmission between equal indices in 3D, whose operator is the
+// propagator e^{i k_z dz} times the identity (T = 1 for ñ_r = ñ_s): its table holds only that
+// value (hi block, then lo block: 2·N entries) and both components are multiplied by it.
 struct PassRec {
   const void* tab;
   int pair;
   int refl;
+  int scalar;
 };
 
 template <typename T>
@@ -213,6 +217,47 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
   constexpr int U = 4;                   // points per thread whose table values load together
   for (int j = 0; j < npass; ++j) {
     const cx<T>* m = static_cast<const cx<T>*>(ps[j].tab);
+    if constexpr (sizeof(T) != sizeof(double)) {
+      if (ps[j].scalar) {  // propagator only: two table values per point
+        for (int base = tid; base < ny * cols; base += U * nt) {
+          cx<T> tv[U][2];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int idx = base + u * nt;
+            const int xc = idx / ny, y = idx - xc * ny;
+            if (idx < ny * cols && x0 + xc < nx) {
+              const long long q = static_cast<long long>(x0 + xc) * ny + y;
+              tv[u][0] = m[q];
+              tv[u][1] = m[n + q];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int idx = base + u * nt;
+            if (idx >= ny * cols) break;
+            const int xc = idx / ny, y = idx - xc * ny;
+            const int sidx = y * cols + xc;
+            if (x0 + xc >= nx) {
+              wbuf[2 * sidx] = cx<T>{0, 0};
+              wbuf[2 * sidx + 1] = cx<T>{0, 0};
+              continue;
+            }
+            wbuf[2 * sidx] = pmul(sbuf[2 * sidx], tv[u][0], tv[u][1]);
+            wbuf[2 * sidx + 1] = pmul(sbuf[2 * sidx + 1], tv[u][0], tv[u][1]);
+          }
+        }
+        __syncthreads();
+        fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
+        cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
+        for (int idx = tid; idx < tile; idx += nt) {
+          const int xc = idx / run, rem = idx - xc * run;
+          const int x = x0 + xc;
+          if (x < nx) w[static_cast<long long>(x) * run + rem] = wbuf[((rem >> 1) * cols + xc) * 2 + (rem & 1)];
+        }
+        __syncthreads();
+        continue;
+      }
+    }
     for (int base = tid; base < ny * cols; base += U * nt) {
       cx<T> tv[U][kB];
 #pragma unroll
@@ -359,9 +404,10 @@ __global__ void k_convert(cx<To>* dst, const cx<From>* src, long long count) {
 
 // Operator table of one (kind, ñ_r, ñ_s): entry q is mode (x, y) = (q mod nx, q div nx), or with
 // `transposed` (3D solves, read column by column) (q div ny, q mod ny).
+// `scalar` (complex64, equal indices): only m00 = e^{i k_z dz}/N, hi block then lo block.
 template <typename T>
 __global__ void k_build_table(cx<T>* out, int kind, cd nr, cd ns, int ny, int nx, double dy,
-                              double dx, double k0, double dz, int transposed) {
+                              double dx, double k0, double dz, int transposed, int scalar) {
   const long long n = static_cast<long long>(ny) * nx;
   const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (q >= n) return;
@@ -371,6 +417,15 @@ __global__ void k_build_table(cx<T>* out, int kind, cd nr, cd ns, int ny, int nx
   const double ky = fftfreq(yi, ny, dy);
   cd m[3];
   operator_matrix(kind, kx, ky, nr, ns, k0, dz, m);
+  if constexpr (sizeof(T) != sizeof(double)) {
+    if (scalar) {
+      const cd v = m[0] / static_cast<double>(n);
+      const cf hi = cast<float>(v);
+      out[q] = hi;
+      out[n + q] = cf{static_cast<float>(v.re - hi.re), static_cast<float>(v.im - hi.im)};
+      return;
+    }
+  }
   for (int e = 0; e < 3; ++e) {
     if constexpr (sizeof(T) == sizeof(double)) {
       out[e * n + q] = m[e];

@@ -62,7 +62,8 @@ class PlaneSolver final : public Solver {
   void setup();
   // per-step pairs, pair-id planes and interface lists from uint8 labels on the device
   void device_steps(const std::uint8_t* labels_u8, const std::vector<int>& host_of);
-  const C* table(int kind, cd nr, cd ns);
+  // operator table of (kind, ñ_r, ñ_s); scalar: the complex64 propagator-only table
+  const C* table(int kind, cd nr, cd ns, bool scalar = false);
   // pass records of all steps on the device (forward, and backward when with_backward)
   void ensure_passes(bool with_backward);
   // x_ready: xbuf_ already holds the x transform of `in` (3D, fused into the previous step);
@@ -441,7 +442,11 @@ void PlaneSolver<T>::setup() {
   }
   // operator tables of the forward transmission (all runs need them)
   for (std::size_t p = 0; p < in_.nz; ++p)
-    for (auto& pr : steps_[p].pairs) table(kFwdT, index_of(pr.first), index_of(pr.second));
+    for (auto& pr : steps_[p].pairs) {
+      const cd nr = index_of(pr.first), ns = index_of(pr.second);
+      const bool same = nr.re == ns.re && nr.im == ns.im;
+      table(kFwdT, nr, ns, sizeof(T) != sizeof(double) && !is2d() && same);
+    }
   // Born: potential V = 2ñ₀k₀²δn per host slab, full-plane source stores
   if (!hosts_.empty()) {
     pot_.alloc(hosts_.size() * nn, stream_);
@@ -575,14 +580,14 @@ void PlaneSolver<T>::device_steps(const std::uint8_t* labels_u8, const std::vect
 }
 
 template <typename T>
-const cx<T>* PlaneSolver<T>::table(int kind, cd nr, cd ns) {
-  auto key = std::make_tuple(kind, nr.re, nr.im, ns.re, ns.im);
+const cx<T>* PlaneSolver<T>::table(int kind, cd nr, cd ns, bool scalar) {
+  auto key = std::make_tuple(kind + (scalar ? 8 : 0), nr.re, nr.im, ns.re, ns.im);
   auto it = tables_.find(key);
   if (it != tables_.end()) return it->second.ptr;
-  DevBuf<C> t(table_blocks<T>() * n(), stream_);
+  DevBuf<C> t((scalar ? 2 : table_blocks<T>()) * n(), stream_);
   launch(k_build_table<T>, dim3(ceil_div(n(), kThreads)), dim3(kThreads), 0, t.ptr, kind, nr, ns,
          static_cast<int>(in_.ny), static_cast<int>(in_.nx), in_.dy, in_.dx, in_.k0, in_.dz,
-         is2d() ? 0 : 1);
+         is2d() ? 0 : 1, scalar ? 1 : 0);
   const C* ptr = t.ptr;
   tables_.emplace(key, std::move(t));
   return ptr;
@@ -616,7 +621,10 @@ void PlaneSolver<T>::ensure_passes(bool with_backward) {
           const bool same = nr.re == ns.re && nr.im == ns.im;
           if (pass == 1 && same) continue;
           const int kind = pass == 0 ? (backward ? kBwdT : kFwdT) : (backward ? kBwdR : kFwdR);
-          host.push_back(PassRec{table(kind, nr, ns), static_cast<int>(i), pass});
+          // complex64 3D transmissions between equal indices: T = 1, the propagator alone
+          const bool scalar = sizeof(T) != sizeof(double) && !is2d() && pass == 0 && same;
+          host.push_back(PassRec{table(kind, nr, ns, scalar), static_cast<int>(i), pass,
+                                 scalar ? 1 : 0});
           ++(pass == 0 ? pass_nt_[d][s] : pass_nr_[d][s]);
         }
       }
