@@ -41,9 +41,9 @@ COUNT, SEED = 256, 4
 REDUCED: dict = {}  # set by --reduced (profiling runs); empty for the benchmark itself
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # SMs × FP32 lanes × FMA × max clock
 # DRAM bytes (read + write) of the class kernels of one batched run of this workload, summed
-# over the classes, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, kernel
-# variants of the autotuner); the fields stay on chip, this is mostly pair-id planes of the
-# longest lines that L2 cannot hold
+# over the classes (dram__bytes_read.sum + dram__bytes_write.sum of an earlier full-workload
+# capture of these kernels; the reduced-case capture gives a few KB per slab step); the fields
+# stay on chip, this is mostly pair-id planes of the longest lines that L2 cannot hold
 TRAFFIC_PER_RUN_BYTES = 1.82e9
 
 
@@ -436,8 +436,9 @@ def run_ours(args) -> None:
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS,
                      "unit": "TFLOP/s", "frac": achieved / FP32_NOMINAL_TFLOPS,
                      "traffic": TRAFFIC_PER_RUN_BYTES if not REDUCED else None,
-                     "traffic_note": "bytes per batched run (all class kernels), one ncu capture of "
-                                     "this workload with the autotuner's kernel variants",
+                     "traffic_note": "bytes per batched run (all class kernels), from an earlier "
+                                     "full-workload ncu capture of these kernels; a reduced-case "
+                                     "capture gives ~13 KB per 8192-point slab step",
                      "note": "shared-memory FFT: SIMT FP32 and shared-memory bound, no tensor "
                              "cores (FFT is not a dense contraction); peak = nominal FP32 "
                              "(no measured FP32 peak in MEASURED_PEAKS.json)",
