@@ -15,6 +15,7 @@
 // k_rows_select (inverse x transform + epilogue).
 #pragma once
 
+#include "bulk.cuh"
 #include "fft.cuh"
 #include "interface.cuh"
 
@@ -181,6 +182,7 @@ struct ColStep {
   cx<T>* work;          // npass planes, transposed like `in`
   cx<T>* spec_out;      // full spectrum F{e} (N, 2) row-major, or null
   int ny, nx, cols;
+  int* status;          // k_cols_step_bulk: set to 1 when a bulk copy does not complete in time
 };
 
 // y transform of a tile of `cols` columns, then per pass: W = M·Ŝ (2×2), inverse y transform,
@@ -300,6 +302,105 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
   }
 }
 
+// k_cols_step for one column per CTA, with the column and the passes' table runs brought into
+// shared memory by bulk copies (cp.async.bulk, completed on mbarriers). Passes go in groups of G:
+// the G spectral products share one inverse transform (smem [y][g][c], 2·G lanes), and the
+// tables of the next group load while the current group transforms and stores. Needs an even
+// ny (16-byte runs) and 16-byte aligned planes and tables (the host checks).
+// smem: column [y][c] (2·ny), work tile (2·G·ny), G table buffers (blocks × ny each), 2 mbarriers.
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, const PassRec* __restrict__ ps, int npass,
+                                 FftPlan plan, const Tw<T>* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kB = table_blocks<T>();
+  const int ny = a.ny, G = a.cols;  // a.cols carries the group size for this kernel
+  const long long n = static_cast<long long>(ny) * a.nx;
+  cx<T>* sbuf = reinterpret_cast<cx<T>*>(smem_raw);
+  cx<T>* wbuf = sbuf + 2 * ny;
+  cx<T>* tbuf = wbuf + 2 * G * ny;  // table of group slot g at tbuf + g·kB·ny
+  std::uint64_t* mbar = reinterpret_cast<std::uint64_t*>(tbuf + G * kB * ny);
+  const int x = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const unsigned run_bytes = 2u * ny * sizeof(cx<T>);
+  auto scalar = [&](int j) { return sizeof(T) != sizeof(double) && ps[j].scalar; };
+  auto issue_group = [&](int j0) {  // one thread: the tables of passes j0 … j0 + G − 1
+    const int g = min(G, npass - j0);
+    unsigned bytes = 0;
+    for (int gi = 0; gi < g; ++gi) bytes += (scalar(j0 + gi) ? 2 : kB) * ny * sizeof(cx<T>);
+    bulk_expect(mbar + 1, bytes);
+    for (int gi = 0; gi < g; ++gi) {
+      const cx<T>* m = static_cast<const cx<T>*>(ps[j0 + gi].tab);
+      const int blocks = scalar(j0 + gi) ? 2 : kB;
+      for (int b = 0; b < blocks; ++b)
+        bulk_load(tbuf + (gi * kB + b) * ny, m + b * n + static_cast<long long>(x) * ny,
+                  static_cast<unsigned>(ny * sizeof(cx<T>)), mbar + 1);
+    }
+  };
+  if (tid == 0) {
+    bulk_mbar_init(mbar, 1);
+    bulk_mbar_init(mbar + 1, 1);
+    bulk_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    bulk_expect(mbar, run_bytes);
+    bulk_load(sbuf, a.in + static_cast<long long>(x) * 2 * ny, run_bytes, mbar);
+    if (npass > 0) issue_group(0);
+  }
+  bulk_wait(mbar, 0, a.status);
+  fft_smem<-1>(sbuf, plan, tw, 2, tid, nt);
+  if (a.spec_out)
+    for (int i = tid; i < 2 * ny; i += nt)
+      a.spec_out[(static_cast<long long>(i >> 1) * a.nx + x) * 2 + (i & 1)] = sbuf[i];
+  unsigned phase = 0;
+  for (int j0 = 0; j0 < npass; j0 += G) {
+    const int g = min(G, npass - j0);
+    bulk_wait(mbar + 1, phase, a.status);
+    phase ^= 1u;
+    for (int idx = tid; idx < G * ny; idx += nt) {
+      const int y = idx / G, gi = idx - y * G;
+      cx<T> w0{0, 0}, w1{0, 0};
+      if (gi < g) {
+        const cx<T>* tb = tbuf + gi * kB * ny;
+        const cx<T> s0 = sbuf[2 * y], s1 = sbuf[2 * y + 1];
+        bool done = false;
+        if constexpr (sizeof(T) != sizeof(double)) {
+          if (scalar(j0 + gi)) {
+            w0 = pmul(s0, tb[y], tb[ny + y]);
+            w1 = pmul(s1, tb[y], tb[ny + y]);
+            done = true;
+          }
+        }
+        if (!done) {
+          cx<T> tv[kB];
+#pragma unroll
+          for (int e = 0; e < kB; ++e) tv[e] = tb[e * ny + y];
+          w0 = tmul_v(s0, tv, 0) + tmul_v(s1, tv, 1);
+          w1 = tmul_v(s0, tv, 1) + tmul_v(s1, tv, 2);
+        }
+      }
+      wbuf[(y * G + gi) * 2] = w0;
+      wbuf[(y * G + gi) * 2 + 1] = w1;
+    }
+    __syncthreads();
+    // the table buffers are free: the next group's tables load during this group's transform
+    if (tid == 0 && j0 + G < npass) issue_group(j0 + G);
+    fft_smem<+1>(wbuf, plan, tw, 2 * G, tid, nt);
+    for (int idx = tid; idx < g * 2 * ny; idx += nt) {  // per pass one contiguous column
+      const int gi = idx / (2 * ny), i = idx - gi * 2 * ny;
+      a.work[static_cast<long long>(j0 + gi) * 2 * n + static_cast<long long>(x) * 2 * ny + i] =
+          wbuf[((i >> 1) * G + gi) * 2 + (i & 1)];
+    }
+    __syncthreads();
+  }
+}
+
+// shared memory of k_cols_step_bulk with passes in groups of g
+template <typename T>
+constexpr std::size_t cols_bulk_smem(int ny, int g) {
+  return (static_cast<std::size_t>(2 + 2 * g) * ny + static_cast<std::size_t>(g) * table_blocks<T>() * ny) *
+             sizeof(cx<T>) + 2 * sizeof(std::uint64_t);
+}
+
 template <typename T>
 struct RowSelect {
   const cx<T>* work;        // npass planes after the inverse y transform, transposed (x-major)
@@ -313,6 +414,7 @@ struct RowSelect {
   cx<T>* xnext;             // or null: also the x transform of the output rows (the next step's
                             // first transform, fused here), stored transposed
   int ny, nx, rows;
+  int group;                // passes per inverse transform (shared memory holds group planes' rows)
   T inv_n;
 };
 
@@ -329,34 +431,44 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
   const int tid = threadIdx.x, nt = blockDim.x;
   const int per_row = nx * 2, total = rows * per_row;
   const int k0 = a.iface ? a.rowoff[y0] : 0, k1 = a.iface ? a.rowoff[y0 + here] : 0;
-  for (int j = 0; j < npass; ++j) {
-    const cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
-    for (int idx = tid; idx < total; idx += nt) {  // per x a run of `rows` rows × 2 (transposed)
-      const int x = idx / (2 * rows), rem = idx - x * 2 * rows;
-      buf[x * rows * 2 + rem] =
-          (rem >> 1) < here ? w[(static_cast<long long>(x) * ny + y0) * 2 + rem] : cx<T>{0, 0};
+  // passes in groups of G: the G work planes' rows share one inverse transform, smem
+  // [x][row][g][c] (G·2·rows lanes), so a multi-pass step pays the transform's latency per group
+  const int G = a.group;
+  const int lanes = 2 * rows * G;
+  for (int j0 = 0; j0 < npass; j0 += G) {
+    const int g = min(G, npass - j0);
+    for (int idx = tid; idx < G * total; idx += nt) {  // per (x, pass) a run of rows × 2
+      const int gi = idx / total, r = idx - gi * total;
+      const int x = r / (2 * rows), rem = r - x * 2 * rows;
+      cx<T> v{0, 0};
+      if (gi < g && (rem >> 1) < here)
+        v = a.work[static_cast<long long>(j0 + gi) * 2 * n + (static_cast<long long>(x) * ny + y0) * 2 + rem];
+      buf[(x * rows + (rem >> 1)) * 2 * G + gi * 2 + (rem & 1)] = v;
     }
     __syncthreads();
-    fft_smem<+1>(buf, plan, tw, 2 * rows, tid, nt);
-    const int pair = ps[j].pair;
-    if (!ps[j].refl) {
-      for (int idx = tid; idx < here * per_row; idx += nt) {
-        const int row = idx / per_row, rem = idx - row * per_row;
-        const int x = rem >> 1, c = rem & 1;
-        const long long q = static_cast<long long>(y0 + row) * nx + x;
-        if (!a.pid || a.pid[q] == pair) {
-          cx<T> v = buf[(x * rows + row) * 2 + c] * a.inv_n;
-          if (a.mask) v = mmul(v, a.mask, q, n);
-          a.out[2 * q + c] = v;
+    fft_smem<+1>(buf, plan, tw, lanes, tid, nt);
+    for (int gi = 0; gi < g; ++gi) {
+      const int j = j0 + gi;
+      const int pair = ps[j].pair;
+      if (!ps[j].refl) {
+        for (int idx = tid; idx < here * per_row; idx += nt) {
+          const int row = idx / per_row, rem = idx - row * per_row;
+          const int x = rem >> 1, c = rem & 1;
+          const long long q = static_cast<long long>(y0 + row) * nx + x;
+          if (!a.pid || a.pid[q] == pair) {
+            cx<T> v = buf[(x * rows + row) * 2 * G + gi * 2 + c] * a.inv_n;
+            if (a.mask) v = mmul(v, a.mask, q, n);
+            a.out[2 * q + c] = v;
+          }
         }
-      }
-    } else {
-      for (int k = k0 + tid; k < k1; k += nt) {
-        const int q = a.iface[k];
-        if (a.pid && a.pid[q] != pair) continue;
-        const int row = q / nx - y0, x = q - (q / nx) * nx;
-        a.refl_out[2 * k] = buf[(x * rows + row) * 2] * a.inv_n;
-        a.refl_out[2 * k + 1] = buf[(x * rows + row) * 2 + 1] * a.inv_n;
+      } else {
+        for (int k = k0 + tid; k < k1; k += nt) {
+          const int q = a.iface[k];
+          if (a.pid && a.pid[q] != pair) continue;
+          const int row = q / nx - y0, x = q - (q / nx) * nx;
+          a.refl_out[2 * k] = buf[(x * rows + row) * 2 * G + gi * 2] * a.inv_n;
+          a.refl_out[2 * k + 1] = buf[(x * rows + row) * 2 * G + gi * 2 + 1] * a.inv_n;
+        }
       }
     }
     __syncthreads();

@@ -43,6 +43,7 @@ struct StepInfo {
 struct LaunchShape {
   int rows = 1, threads = 32;
   std::size_t smem = 0;
+  int group = 1;  // passes per inverse transform (row kernel of a 3D step)
 };
 
 template <typename T>
@@ -130,6 +131,9 @@ class PlaneSolver final : public Solver {
   int sms_ = 148;
   LaunchShape rows2_, rows3_, sel_, cols1_, cols2_, cols3_;
   std::int64_t launches_ = 0, gmres_applies_ = 0;
+  bool cols_bulk_ = false;  // 3D column kernel with bulk copies (k_cols_step_bulk)
+  int cols_bulk_threads_ = 256, cols_bulk_group_ = 1;
+  DevBuf<int> status_;      // set by a kernel whose bounded wait gave up
   DevBuf<PassRec> pass_pool_;
   std::vector<long long> pass_off_[2];
   std::vector<int> pass_nt_[2], pass_nr_[2];
@@ -160,10 +164,16 @@ LaunchShape PlaneSolver<T>::step_rows_shape() const {
   rows = std::min<int>(rows, static_cast<int>(in_.ny));
   while (rows > 1 && (rows * row_bytes > 98304 || threads_needed(hx_.plan, rows * 2) > kPlaneThreads)) --rows;
   s.rows = rows;
-  s.threads = std::max(256, threads_needed(hx_.plan, rows * 2));
-  if (s.threads > kPlaneThreads || rows * row_bytes > 227 * 1024)
+  if (threads_needed(hx_.plan, rows * 2) > kPlaneThreads || rows * row_bytes > 227 * 1024)
     throw invalid_argument("nx too large for the row transform");
-  s.smem = rows * row_bytes;
+  // passes per inverse transform: up to 4, while the threads and shared memory allow it
+  int g = std::min(4, std::max(1, max_pass_));
+  while (g > 1 && (threads_needed(hx_.plan, rows * 2 * g) > kPlaneThreads ||
+                   static_cast<std::size_t>(g) * rows * row_bytes > 200 * 1024))
+    g = g > 2 ? 2 : 1;
+  s.group = g;
+  s.threads = std::max(256, threads_needed(hx_.plan, rows * 2 * g));
+  s.smem = static_cast<std::size_t>(g) * rows * row_bytes;
   return s;
 }
 
@@ -432,11 +442,27 @@ void PlaneSolver<T>::setup() {
     cols1_ = cols_shape(2, 1);
     cols2_ = cols_shape(2, 2);
     cols3_ = cols_shape(3, 1);
+    // the bulk-copy column kernel needs 16-byte runs (even ny) and its buffers in shared memory;
+    // BWPM_COLS=plain selects the plain-load kernel
+    const char* ck = std::getenv("BWPM_COLS");
+    const int nyi = static_cast<int>(in_.ny);
+    cols_bulk_group_ = std::min(4, std::max(1, max_pass_));
+    while (cols_bulk_group_ > 1 && (cols_bulk_smem<T>(nyi, cols_bulk_group_) > 200 * 1024 ||
+                                    threads_needed(hy_.plan, 2 * cols_bulk_group_) > kPlaneThreads))
+      cols_bulk_group_ = cols_bulk_group_ > 2 ? 2 : 1;
+    cols_bulk_ = in_.ny % 2 == 0 && cols_bulk_smem<T>(nyi, cols_bulk_group_) <= 200 * 1024 &&
+                 threads_needed(hy_.plan, 2 * cols_bulk_group_) <= kPlaneThreads &&
+                 !(ck && std::strcmp(ck, "plain") == 0);
+    cols_bulk_threads_ =
+        std::min(kPlaneThreads, std::max(256, threads_needed(hy_.plan, 2 * cols_bulk_group_)));
+    status_.alloc(1, stream_);
+    check_cuda(cudaMemsetAsync(status_.ptr, 0, sizeof(int), stream_), "memset");
     xbuf_.alloc(2 * nn, stream_);
     work_.alloc(static_cast<std::size_t>(max_pass_) * 2 * nn, stream_);
     for (auto k : {(const void*)k_rows_fft<-1, T>, (const void*)k_rows_fft<1, T>,
                    (const void*)k_rows_fft<-1, T, true>,
-                   (const void*)k_cols_step<T>, (const void*)k_rows_select<T>,
+                   (const void*)k_cols_step<T>, (const void*)k_cols_step_bulk<T>,
+                   (const void*)k_rows_select<T>,
                    (const void*)k_cols_fft<-1, T>, (const void*)k_cols_fft<1, T>})
       check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
   }
@@ -667,10 +693,17 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   if (!x_ready)  // the x transform of the step's input, stored transposed for the column kernel
     launch(k_rows_fft<-1, T, true>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, in,
            xbuf_.ptr, ny, nx, 2, sel_.rows, hx_.plan, tw_x_.ptr);
-  const LaunchShape& cs = npass > 1 ? cols2_ : cols1_;
-  ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cs.rows};
-  launch(k_cols_step<T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem, c, ps, npass, hy_.plan,
-         tw_y_.ptr);
+  if (cols_bulk_) {
+    ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cols_bulk_group_,
+                 status_.ptr};
+    launch(k_cols_step_bulk<T>, dim3(nx), dim3(cols_bulk_threads_),
+           cols_bulk_smem<T>(ny, cols_bulk_group_), c, ps, npass, hy_.plan, tw_y_.ptr);
+  } else {
+    const LaunchShape& cs = npass > 1 ? cols2_ : cols1_;
+    ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cs.rows, nullptr};
+    launch(k_cols_step<T>, dim3(ceil_div(nx, cs.rows)), dim3(cs.threads), cs.smem, c, ps, npass,
+           hy_.plan, tw_y_.ptr);
+  }
   RowSelect<T> r;
   r.work = work_.ptr;
   r.out = out;
@@ -684,6 +717,7 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   r.ny = ny;
   r.nx = nx;
   r.rows = sel_.rows;
+  r.group = sel_.group;
   r.inv_n = inv_n;
   launch(k_rows_select<T>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, r, ps, npass,
          hx_.plan, tw_x_.ptr);
@@ -996,6 +1030,14 @@ void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* ke
   }
   out.stored_values = iterations > 0 ? 2 * iface_total_ : 0;
   check_cuda(cudaStreamSynchronize(stream_), "synchronize");
+  if (status_.ptr) {
+    int st = 0;
+    check_cuda(cudaMemcpy(&st, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost), "status");
+    if (st) {
+      check_cuda(cudaMemset(status_.ptr, 0, sizeof(int)), "status");
+      throw std::runtime_error("a bulk copy of the 3D slab step did not complete in time");
+    }
+  }
 }
 
 template <typename T>

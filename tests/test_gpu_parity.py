@@ -218,3 +218,23 @@ def test_device_setup_equals_host_setup(core, monkeypatch, prefix, iters, precis
         assert np.array_equal(a["forward"][q], b["forward"][q])
         assert np.array_equal(a["backward"][q], b["backward"][q])
     assert a["stored_values"] == b["stored_values"]
+
+
+@pytest.mark.parametrize("prefix,iters", [("volume2.", 2), ("volume3.", 2), ("backscatter.", 3)])
+@pytest.mark.parametrize("precision", [64, 32])
+def test_bulk_column_kernel_equals_plain_loads(core, monkeypatch, prefix, iters, precision):
+    """The 3D column kernel that stages columns and tables with bulk copies and groups passes
+    (k_cols_step_bulk) gives the same bits as the plain-load kernel (BWPM_COLS=plain)."""
+    d = load_npz("random_volumes.npz")
+    args, field, fl = volume_case(d, prefix)
+    assert int(args[0]) % 2 == 0  # even ny: the bulk path applies
+    out = {}
+    for mode in ("plain", "bulk"):
+        monkeypatch.setenv("BWPM_COLS", mode)
+        out[mode] = core.CudaSolver(*args, 0, fluctuation=fl, precision=precision).run(
+            field, iters, [0, 5])
+    a, b = out["plain"], out["bulk"]
+    for key in ("transmitted", "reflected"):
+        assert np.array_equal(a[key], b[key]), key
+    for q in (0, 5):
+        assert np.array_equal(a["forward"][q], b["forward"][q])
