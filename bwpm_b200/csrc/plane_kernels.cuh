@@ -302,88 +302,90 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
   }
 }
 
-// k_cols_step for one column per CTA, with the column and the passes' table runs brought into
-// shared memory by bulk copies (cp.async.bulk, completed on mbarriers). Passes go in groups of G:
-// the G spectral products share one inverse transform (smem [y][g][c], 2·G lanes), and the
-// tables of the next group load while the current group transforms and stores. Needs an even
-// ny (16-byte runs) and 16-byte aligned planes and tables (the host checks).
-// smem: column [y][c] (2·ny), work tile (2·G·ny), G table buffers (blocks × ny each), 2 mbarriers.
+// k_cols_step for one column per CTA: the column is brought into shared memory by one bulk copy
+// (cp.async.bulk on an mbarrier, bounded wait), and the passes go in groups of G whose spectral
+// products share one inverse transform (smem [y][g][c], 2·G lanes), each thread loading the
+// table values of several points at once. The tables stay in global memory (L2): staging them in
+// shared memory as well took the kernel to one CTA per SM and made it slower. Needs an even ny
+// (16-byte runs) and 16-byte aligned planes (the host checks).
+// smem: column [y][c] (2·ny), work tile (2·G·ny), one mbarrier.
 template <typename T>
 __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, const PassRec* __restrict__ ps, int npass,
                                  FftPlan plan, const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kB = table_blocks<T>();
+  constexpr int U = 4;  // points per thread whose table values load together
   const int ny = a.ny, G = a.cols;  // a.cols carries the group size for this kernel
   const long long n = static_cast<long long>(ny) * a.nx;
   cx<T>* sbuf = reinterpret_cast<cx<T>*>(smem_raw);
   cx<T>* wbuf = sbuf + 2 * ny;
-  cx<T>* tbuf = wbuf + 2 * G * ny;  // table of group slot g at tbuf + g·kB·ny
-  std::uint64_t* mbar = reinterpret_cast<std::uint64_t*>(tbuf + G * kB * ny);
+  std::uint64_t* mbar = reinterpret_cast<std::uint64_t*>(wbuf + 2 * G * ny);
   const int x = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const unsigned run_bytes = 2u * ny * sizeof(cx<T>);
-  auto scalar = [&](int j) { return sizeof(T) != sizeof(double) && ps[j].scalar; };
-  auto issue_group = [&](int j0) {  // one thread: the tables of passes j0 … j0 + G − 1
-    const int g = min(G, npass - j0);
-    unsigned bytes = 0;
-    for (int gi = 0; gi < g; ++gi) bytes += (scalar(j0 + gi) ? 2 : kB) * ny * sizeof(cx<T>);
-    bulk_expect(mbar + 1, bytes);
-    for (int gi = 0; gi < g; ++gi) {
-      const cx<T>* m = static_cast<const cx<T>*>(ps[j0 + gi].tab);
-      const int blocks = scalar(j0 + gi) ? 2 : kB;
-      for (int b = 0; b < blocks; ++b)
-        bulk_load(tbuf + (gi * kB + b) * ny, m + b * n + static_cast<long long>(x) * ny,
-                  static_cast<unsigned>(ny * sizeof(cx<T>)), mbar + 1);
-    }
-  };
   if (tid == 0) {
     bulk_mbar_init(mbar, 1);
-    bulk_mbar_init(mbar + 1, 1);
     bulk_fence_init();
   }
   __syncthreads();
   if (tid == 0) {
     bulk_expect(mbar, run_bytes);
     bulk_load(sbuf, a.in + static_cast<long long>(x) * 2 * ny, run_bytes, mbar);
-    if (npass > 0) issue_group(0);
   }
   bulk_wait(mbar, 0, a.status);
   fft_smem<-1>(sbuf, plan, tw, 2, tid, nt);
   if (a.spec_out)
     for (int i = tid; i < 2 * ny; i += nt)
       a.spec_out[(static_cast<long long>(i >> 1) * a.nx + x) * 2 + (i & 1)] = sbuf[i];
-  unsigned phase = 0;
   for (int j0 = 0; j0 < npass; j0 += G) {
     const int g = min(G, npass - j0);
-    bulk_wait(mbar + 1, phase, a.status);
-    phase ^= 1u;
-    for (int idx = tid; idx < G * ny; idx += nt) {
-      const int y = idx / G, gi = idx - y * G;
-      cx<T> w0{0, 0}, w1{0, 0};
-      if (gi < g) {
-        const cx<T>* tb = tbuf + gi * kB * ny;
-        const cx<T> s0 = sbuf[2 * y], s1 = sbuf[2 * y + 1];
-        bool done = false;
-        if constexpr (sizeof(T) != sizeof(double)) {
-          if (scalar(j0 + gi)) {
-            w0 = pmul(s0, tb[y], tb[ny + y]);
-            w1 = pmul(s1, tb[y], tb[ny + y]);
-            done = true;
+    for (int base = tid; base < G * ny; base += U * nt) {
+      cx<T> tv[U][kB];
+      bool sc[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {  // the table values of U points in flight at once
+        const int idx = base + u * nt;
+        const int gi = idx / ny, y = idx - gi * ny;
+        sc[u] = false;
+        if (idx < G * ny && gi < g) {
+          const PassRec pr = ps[j0 + gi];
+          const cx<T>* m = static_cast<const cx<T>*>(pr.tab);
+          const long long q = static_cast<long long>(x) * ny + y;
+          sc[u] = sizeof(T) != sizeof(double) && pr.scalar;
+          if (sc[u]) {
+            tv[u][0] = m[q];
+            tv[u][1] = m[n + q];
+          } else {
+#pragma unroll
+            for (int b = 0; b < kB; ++b) tv[u][b] = m[b * n + q];
           }
         }
-        if (!done) {
-          cx<T> tv[kB];
-#pragma unroll
-          for (int e = 0; e < kB; ++e) tv[e] = tb[e * ny + y];
-          w0 = tmul_v(s0, tv, 0) + tmul_v(s1, tv, 1);
-          w1 = tmul_v(s0, tv, 1) + tmul_v(s1, tv, 2);
-        }
       }
-      wbuf[(y * G + gi) * 2] = w0;
-      wbuf[(y * G + gi) * 2 + 1] = w1;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + u * nt;
+        if (idx >= G * ny) break;
+        const int gi = idx / ny, y = idx - gi * ny;
+        cx<T> w0{0, 0}, w1{0, 0};
+        if (gi < g) {
+          const cx<T> s0 = sbuf[2 * y], s1 = sbuf[2 * y + 1];
+          bool done = false;
+          if constexpr (sizeof(T) != sizeof(double)) {
+            if (sc[u]) {
+              w0 = pmul(s0, tv[u][0], tv[u][1]);
+              w1 = pmul(s1, tv[u][0], tv[u][1]);
+              done = true;
+            }
+          }
+          if (!done) {
+            w0 = tmul_v(s0, tv[u], 0) + tmul_v(s1, tv[u], 1);
+            w1 = tmul_v(s0, tv[u], 1) + tmul_v(s1, tv[u], 2);
+          }
+        }
+        wbuf[(y * G + gi) * 2] = w0;
+        wbuf[(y * G + gi) * 2 + 1] = w1;
+      }
     }
     __syncthreads();
-    // the table buffers are free: the next group's tables load during this group's transform
-    if (tid == 0 && j0 + G < npass) issue_group(j0 + G);
     fft_smem<+1>(wbuf, plan, tw, 2 * G, tid, nt);
     for (int idx = tid; idx < g * 2 * ny; idx += nt) {  // per pass one contiguous column
       const int gi = idx / (2 * ny), i = idx - gi * 2 * ny;
@@ -397,8 +399,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
 // shared memory of k_cols_step_bulk with passes in groups of g
 template <typename T>
 constexpr std::size_t cols_bulk_smem(int ny, int g) {
-  return (static_cast<std::size_t>(2 + 2 * g) * ny + static_cast<std::size_t>(g) * table_blocks<T>() * ny) *
-             sizeof(cx<T>) + 2 * sizeof(std::uint64_t);
+  return static_cast<std::size_t>(2 + 2 * g) * ny * sizeof(cx<T>) + sizeof(std::uint64_t);
 }
 
 template <typename T>

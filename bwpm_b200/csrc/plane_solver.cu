@@ -166,10 +166,11 @@ LaunchShape PlaneSolver<T>::step_rows_shape() const {
   s.rows = rows;
   if (threads_needed(hx_.plan, rows * 2) > kPlaneThreads || rows * row_bytes > 227 * 1024)
     throw invalid_argument("nx too large for the row transform");
-  // passes per inverse transform: up to 4, while the threads and shared memory allow it
+  // passes per inverse transform: up to 4, while the threads allow it and the shared memory
+  // leaves room for at least 3 CTAs per SM (these kernels are latency-bound)
   int g = std::min(4, std::max(1, max_pass_));
   while (g > 1 && (threads_needed(hx_.plan, rows * 2 * g) > kPlaneThreads ||
-                   static_cast<std::size_t>(g) * rows * row_bytes > 200 * 1024))
+                   static_cast<std::size_t>(g) * rows * row_bytes > 64 * 1024))
     g = g > 2 ? 2 : 1;
   s.group = g;
   s.threads = std::max(256, threads_needed(hx_.plan, rows * 2 * g));
@@ -446,8 +447,10 @@ void PlaneSolver<T>::setup() {
     // BWPM_COLS=plain selects the plain-load kernel
     const char* ck = std::getenv("BWPM_COLS");
     const int nyi = static_cast<int>(in_.ny);
+    // group size: up to 4 passes, keeping shared memory for 4 CTAs per SM (occupancy matters
+    // more than grouping: these kernels are latency-bound)
     cols_bulk_group_ = std::min(4, std::max(1, max_pass_));
-    while (cols_bulk_group_ > 1 && (cols_bulk_smem<T>(nyi, cols_bulk_group_) > 200 * 1024 ||
+    while (cols_bulk_group_ > 1 && (cols_bulk_smem<T>(nyi, cols_bulk_group_) > 56 * 1024 ||
                                     threads_needed(hy_.plan, 2 * cols_bulk_group_) > kPlaneThreads))
       cols_bulk_group_ = cols_bulk_group_ > 2 ? 2 : 1;
     cols_bulk_ = in_.ny % 2 == 0 && cols_bulk_smem<T>(nyi, cols_bulk_group_) <= 200 * 1024 &&
