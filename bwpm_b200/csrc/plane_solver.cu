@@ -9,6 +9,7 @@
 // - selection, mask, reflection gather and sparse source add are fused into the inverse
 //   transform's epilogue; interface pixel lists and source stores are allocated once.
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -156,11 +157,22 @@ LaunchShape PlaneSolver<T>::rows_shape(int ncomp, int rows_max) const {
 
 // Rows per CTA of the slab-step row kernels (2 components): 4 when that still gives a CTA per
 // SM, else 2, so that every transposed run (rows × 16 B in complex64) fills whole 32-byte sectors.
+// Launch-shape override of the 3D step kernels for tuning measurements: BWPM_3D_SHAPE =
+// "rows,row_group,col_group,col_threads,row_threads" (0 keeps a field's default choice).
+inline void shape_override(int (&v)[5]) {
+  for (int& x : v) x = 0;
+  if (const char* e = std::getenv("BWPM_3D_SHAPE"))
+    std::sscanf(e, "%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4]);
+}
+
 template <typename T>
 LaunchShape PlaneSolver<T>::step_rows_shape() const {
   LaunchShape s;
+  int ov[5];
+  shape_override(ov);
   const std::size_t row_bytes = in_.nx * 2 * sizeof(C);
   int rows = static_cast<int>(in_.ny) / 4 >= sms_ ? 4 : 2;
+  if (ov[0] > 0) rows = ov[0];
   rows = std::min<int>(rows, static_cast<int>(in_.ny));
   while (rows > 1 && (rows * row_bytes > 98304 || threads_needed(hx_.plan, rows * 2) > kPlaneThreads)) --rows;
   s.rows = rows;
@@ -168,12 +180,13 @@ LaunchShape PlaneSolver<T>::step_rows_shape() const {
     throw invalid_argument("nx too large for the row transform");
   // passes per inverse transform: up to 4, while the threads allow it and the shared memory
   // leaves room for at least 3 CTAs per SM (these kernels are latency-bound)
-  int g = std::min(4, std::max(1, max_pass_));
+  int g = std::min(ov[1] > 0 ? ov[1] : 4, std::max(1, max_pass_));
   while (g > 1 && (threads_needed(hx_.plan, rows * 2 * g) > kPlaneThreads ||
-                   static_cast<std::size_t>(g) * rows * row_bytes > 64 * 1024))
+                   static_cast<std::size_t>(g) * rows * row_bytes > (ov[1] > 0 ? 200 : 64) * 1024))
     g = g > 2 ? 2 : 1;
   s.group = g;
-  s.threads = std::max(256, threads_needed(hx_.plan, rows * 2 * g));
+  s.threads = std::min(kPlaneThreads,
+                       std::max(ov[4] > 0 ? ov[4] : 256, threads_needed(hx_.plan, rows * 2 * g)));
   s.smem = static_cast<std::size_t>(g) * rows * row_bytes;
   return s;
 }
@@ -449,15 +462,18 @@ void PlaneSolver<T>::setup() {
     const int nyi = static_cast<int>(in_.ny);
     // group size: up to 4 passes, keeping shared memory for 4 CTAs per SM (occupancy matters
     // more than grouping: these kernels are latency-bound)
-    cols_bulk_group_ = std::min(4, std::max(1, max_pass_));
-    while (cols_bulk_group_ > 1 && (cols_bulk_smem<T>(nyi, cols_bulk_group_) > 56 * 1024 ||
-                                    threads_needed(hy_.plan, 2 * cols_bulk_group_) > kPlaneThreads))
+    int ov[5];
+    shape_override(ov);
+    cols_bulk_group_ = std::min(ov[2] > 0 ? ov[2] : 4, std::max(1, max_pass_));
+    while (cols_bulk_group_ > 1 &&
+           (cols_bulk_smem<T>(nyi, cols_bulk_group_) > (ov[2] > 0 ? 200 : 56) * 1024 ||
+            threads_needed(hy_.plan, 2 * cols_bulk_group_) > kPlaneThreads))
       cols_bulk_group_ = cols_bulk_group_ > 2 ? 2 : 1;
     cols_bulk_ = in_.ny % 2 == 0 && cols_bulk_smem<T>(nyi, cols_bulk_group_) <= 200 * 1024 &&
                  threads_needed(hy_.plan, 2 * cols_bulk_group_) <= kPlaneThreads &&
                  !(ck && std::strcmp(ck, "plain") == 0);
-    cols_bulk_threads_ =
-        std::min(kPlaneThreads, std::max(256, threads_needed(hy_.plan, 2 * cols_bulk_group_)));
+    cols_bulk_threads_ = std::min(
+        kPlaneThreads, std::max(ov[3] > 0 ? ov[3] : 256, threads_needed(hy_.plan, 2 * cols_bulk_group_)));
     status_.alloc(1, stream_);
     check_cuda(cudaMemsetAsync(status_.ptr, 0, sizeof(int), stream_), "memset");
     xbuf_.alloc(2 * nn, stream_);
