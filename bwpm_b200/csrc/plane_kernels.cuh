@@ -387,10 +387,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
     }
     __syncthreads();
     fft_smem<+1>(wbuf, plan, tw, 2 * G, tid, nt);
-    for (int idx = tid; idx < g * 2 * ny; idx += nt) {  // per pass one contiguous column
-      const int gi = idx / (2 * ny), i = idx - gi * 2 * ny;
-      a.work[static_cast<long long>(j0 + gi) * 2 * n + static_cast<long long>(x) * 2 * ny + i] =
-          wbuf[((i >> 1) * G + gi) * 2 + (i & 1)];
+    for (int idx = tid; idx < g * ny; idx += nt) {  // per pass one contiguous column, by pixel
+      const int gi = idx / ny, y = idx - gi * ny;
+      st_px(a.work + static_cast<long long>(j0 + gi) * 2 * n + (static_cast<long long>(x) * ny + y) * 2,
+            wbuf[(y * G + gi) * 2], wbuf[(y * G + gi) * 2 + 1]);
     }
     __syncthreads();
   }
@@ -400,6 +400,28 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
 template <typename T>
 constexpr std::size_t cols_bulk_smem(int ny, int g) {
   return static_cast<std::size_t>(2 + 2 * g) * ny * sizeof(cx<T>) + sizeof(std::uint64_t);
+}
+
+// Both components of one pixel (two adjacent complex values, 16-byte aligned in complex64).
+template <typename T>
+__device__ __forceinline__ void ld_px(const cx<T>* p, cx<T>& a, cx<T>& b) {
+  if constexpr (sizeof(T) == sizeof(float)) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a = cx<T>{v.x, v.y};
+    b = cx<T>{v.z, v.w};
+  } else {
+    a = p[0];
+    b = p[1];
+  }
+}
+template <typename T>
+__device__ __forceinline__ void st_px(cx<T>* p, cx<T> a, cx<T> b) {
+  if constexpr (sizeof(T) == sizeof(float)) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.re, a.im, b.re, b.im);
+  } else {
+    p[0] = a;
+    p[1] = b;
+  }
 }
 
 template <typename T>
@@ -430,7 +452,6 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
   const int y0 = blockIdx.x * rows;
   const int here = min(rows, ny - y0);
   const int tid = threadIdx.x, nt = blockDim.x;
-  const int per_row = nx * 2, total = rows * per_row;
   const int k0 = a.iface ? a.rowoff[y0] : 0, k1 = a.iface ? a.rowoff[y0 + here] : 0;
   // passes in groups of G: the G work planes' rows share one inverse transform, smem
   // [x][row][g][c] (G·2·rows lanes), so a multi-pass step pays the transform's latency per group
@@ -438,13 +459,31 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
   const int lanes = 2 * rows * G;
   for (int j0 = 0; j0 < npass; j0 += G) {
     const int g = min(G, npass - j0);
-    for (int idx = tid; idx < G * total; idx += nt) {  // per (x, pass) a run of rows × 2
-      const int gi = idx / total, r = idx - gi * total;
-      const int x = r / (2 * rows), rem = r - x * 2 * rows;
-      cx<T> v{0, 0};
-      if (gi < g && (rem >> 1) < here)
-        v = a.work[static_cast<long long>(j0 + gi) * 2 * n + (static_cast<long long>(x) * ny + y0) * 2 + rem];
-      buf[(x * rows + (rem >> 1)) * 2 * G + gi * 2 + (rem & 1)] = v;
+    // per (pass, x) a run of `rows` pixels (transposed planes); four pixels in flight per thread
+    const int npix = G * rows * nx;
+    for (int base = tid; base < npix; base += 4 * nt) {
+      cx<T> va[4], vb[4];
+      int dst[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = base + u * nt;
+        dst[u] = -1;
+        va[u] = vb[u] = cx<T>{0, 0};
+        if (idx < npix) {
+          const int gi = idx / (rows * nx), r = idx - gi * rows * nx;
+          const int x = r / rows, row = r - x * rows;
+          if (gi < g && row < here)
+            ld_px(a.work + static_cast<long long>(j0 + gi) * 2 * n +
+                      (static_cast<long long>(x) * ny + y0 + row) * 2, va[u], vb[u]);
+          dst[u] = (x * rows + row) * 2 * G + gi * 2;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (dst[u] >= 0) {
+          buf[dst[u]] = va[u];
+          buf[dst[u] + 1] = vb[u];
+        }
     }
     __syncthreads();
     fft_smem<+1>(buf, plan, tw, lanes, tid, nt);
@@ -452,14 +491,17 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
       const int j = j0 + gi;
       const int pair = ps[j].pair;
       if (!ps[j].refl) {
-        for (int idx = tid; idx < here * per_row; idx += nt) {
-          const int row = idx / per_row, rem = idx - row * per_row;
-          const int x = rem >> 1, c = rem & 1;
+        for (int idx = tid; idx < here * nx; idx += nt) {  // per pixel both components
+          const int row = idx / nx, x = idx - row * nx;
           const long long q = static_cast<long long>(y0 + row) * nx + x;
           if (!a.pid || a.pid[q] == pair) {
-            cx<T> v = buf[(x * rows + row) * 2 * G + gi * 2 + c] * a.inv_n;
-            if (a.mask) v = mmul(v, a.mask, q, n);
-            a.out[2 * q + c] = v;
+            const int b = (x * rows + row) * 2 * G + gi * 2;
+            cx<T> v0 = buf[b] * a.inv_n, v1 = buf[b + 1] * a.inv_n;
+            if (a.mask) {
+              v0 = mmul(v0, a.mask, q, n);
+              v1 = mmul(v1, a.mask, q, n);
+            }
+            st_px(a.out + 2 * q, v0, v1);
           }
         }
       } else {
@@ -482,18 +524,19 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
     }
   if (a.xnext) {  // forward x transform of this CTA's output rows (written by this CTA above)
     __syncthreads();
-    for (int idx = tid; idx < total; idx += nt) {
-      const int row = idx / per_row, rem = idx - row * per_row;
-      const int x = rem >> 1, c = rem & 1;
-      buf[(x * rows + row) * 2 + c] =
-          row < here ? a.out[(static_cast<long long>(y0 + row) * nx + x) * 2 + c] : cx<T>{0, 0};
+    for (int idx = tid; idx < rows * nx; idx += nt) {  // per pixel both components
+      const int row = idx / nx, x = idx - row * nx;
+      cx<T> v0{0, 0}, v1{0, 0};
+      if (row < here) ld_px(a.out + (static_cast<long long>(y0 + row) * nx + x) * 2, v0, v1);
+      buf[(x * rows + row) * 2] = v0;
+      buf[(x * rows + row) * 2 + 1] = v1;
     }
     __syncthreads();
     fft_smem<-1>(buf, plan, tw, 2 * rows, tid, nt);
-    const int xrun = here * 2;
-    for (int idx = tid; idx < nx * xrun; idx += nt) {
-      const int x = idx / xrun, rem = idx - x * xrun;
-      a.xnext[(static_cast<long long>(x) * ny + y0) * 2 + rem] = buf[x * rows * 2 + rem];
+    for (int idx = tid; idx < nx * here; idx += nt) {  // transposed: per x a run of `here` pixels
+      const int x = idx / here, row = idx - x * here;
+      st_px(a.xnext + (static_cast<long long>(x) * ny + y0 + row) * 2, buf[(x * rows + row) * 2],
+            buf[(x * rows + row) * 2 + 1]);
     }
   }
 }
