@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
       a.spec_out[(static_cast<long long>(i >> 1) * a.nx + x) * 2 + (i & 1)] = sbuf[i];
   for (int j0 = 0; j0 < npass; j0 += G) {
     const int g = min(G, npass - j0);
-    for (int base = tid; base < G * ny; base += U * nt) {
+    for (int base = tid; base < g * ny; base += U * nt) {
       cx<T> tv[U][kB];
       bool sc[U];
 #pragma unroll
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
         const int idx = base + u * nt;
         const int gi = idx / ny, y = idx - gi * ny;
         sc[u] = false;
-        if (idx < G * ny && gi < g) {
+        if (idx < g * ny) {
           const PassRec pr = ps[j0 + gi];
           const cx<T>* m = static_cast<const cx<T>*>(pr.tab);
           const long long q = static_cast<long long>(x) * ny + y;
@@ -363,10 +363,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int idx = base + u * nt;
-        if (idx >= G * ny) break;
+        if (idx >= g * ny) break;
         const int gi = idx / ny, y = idx - gi * ny;
         cx<T> w0{0, 0}, w1{0, 0};
-        if (gi < g) {
+        {
           const cx<T> s0 = sbuf[2 * y], s1 = sbuf[2 * y + 1];
           bool done = false;
           if constexpr (sizeof(T) != sizeof(double)) {
@@ -381,16 +381,16 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
             w1 = tmul_v(s0, tv[u], 1) + tmul_v(s1, tv[u], 2);
           }
         }
-        wbuf[(y * G + gi) * 2] = w0;
-        wbuf[(y * G + gi) * 2 + 1] = w1;
+        wbuf[(y * g + gi) * 2] = w0;
+        wbuf[(y * g + gi) * 2 + 1] = w1;
       }
     }
     __syncthreads();
-    fft_smem<+1>(wbuf, plan, tw, 2 * G, tid, nt);
+    fft_smem<+1>(wbuf, plan, tw, 2 * g, tid, nt);
     for (int idx = tid; idx < g * ny; idx += nt) {  // per pass one contiguous column, by pixel
       const int gi = idx / ny, y = idx - gi * ny;
       st_px(a.work + static_cast<long long>(j0 + gi) * 2 * n + (static_cast<long long>(x) * ny + y) * 2,
-            wbuf[(y * G + gi) * 2], wbuf[(y * G + gi) * 2 + 1]);
+            wbuf[(y * g + gi) * 2], wbuf[(y * g + gi) * 2 + 1]);
     }
     __syncthreads();
   }
@@ -456,11 +456,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
   // passes in groups of G: the G work planes' rows share one inverse transform, smem
   // [x][row][g][c] (G·2·rows lanes), so a multi-pass step pays the transform's latency per group
   const int G = a.group;
-  const int lanes = 2 * rows * G;
   for (int j0 = 0; j0 < npass; j0 += G) {
-    const int g = min(G, npass - j0);
+    const int g = min(G, npass - j0);  // passes in this group: the transform has 2·rows·g lanes
     // per (pass, x) a run of `rows` pixels (transposed planes); four pixels in flight per thread
-    const int npix = G * rows * nx;
+    const int npix = g * rows * nx;
     for (int base = tid; base < npix; base += 4 * nt) {
       cx<T> va[4], vb[4];
       int dst[4];
@@ -472,10 +471,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
         if (idx < npix) {
           const int gi = idx / (rows * nx), r = idx - gi * rows * nx;
           const int x = r / rows, row = r - x * rows;
-          if (gi < g && row < here)
+          if (row < here)
             ld_px(a.work + static_cast<long long>(j0 + gi) * 2 * n +
                       (static_cast<long long>(x) * ny + y0 + row) * 2, va[u], vb[u]);
-          dst[u] = (x * rows + row) * 2 * G + gi * 2;
+          dst[u] = (x * rows + row) * 2 * g + gi * 2;
         }
       }
 #pragma unroll
@@ -486,7 +485,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
         }
     }
     __syncthreads();
-    fft_smem<+1>(buf, plan, tw, lanes, tid, nt);
+    fft_smem<+1>(buf, plan, tw, 2 * rows * g, tid, nt);
     for (int gi = 0; gi < g; ++gi) {
       const int j = j0 + gi;
       const int pair = ps[j].pair;
@@ -495,7 +494,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
           const int row = idx / nx, x = idx - row * nx;
           const long long q = static_cast<long long>(y0 + row) * nx + x;
           if (!a.pid || a.pid[q] == pair) {
-            const int b = (x * rows + row) * 2 * G + gi * 2;
+            const int b = (x * rows + row) * 2 * g + gi * 2;
             cx<T> v0 = buf[b] * a.inv_n, v1 = buf[b + 1] * a.inv_n;
             if (a.mask) {
               v0 = mmul(v0, a.mask, q, n);
@@ -509,8 +508,8 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
           const int q = a.iface[k];
           if (a.pid && a.pid[q] != pair) continue;
           const int row = q / nx - y0, x = q - (q / nx) * nx;
-          a.refl_out[2 * k] = buf[(x * rows + row) * 2 * G + gi * 2] * a.inv_n;
-          a.refl_out[2 * k + 1] = buf[(x * rows + row) * 2 * G + gi * 2 + 1] * a.inv_n;
+          a.refl_out[2 * k] = buf[(x * rows + row) * 2 * g + gi * 2] * a.inv_n;
+          a.refl_out[2 * k + 1] = buf[(x * rows + row) * 2 * g + gi * 2 + 1] * a.inv_n;
         }
       }
     }
