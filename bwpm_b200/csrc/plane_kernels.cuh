@@ -438,6 +438,7 @@ struct RowSelect {
                             // first transform, fused here), stored transposed
   int ny, nx, rows;
   int group;                // passes per inverse transform (shared memory holds group planes' rows)
+  int store_out;            // with xnext on a single-pass step: 0 when nothing reads `out` later
   T inv_n;
 };
 
@@ -456,7 +457,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
   // passes in groups of G: the G work planes' rows share one inverse transform, smem
   // [x][row][g][c] (G·2·rows lanes), so a multi-pass step pays the transform's latency per group
   const int G = a.group;
-  for (int j0 = 0; j0 < npass; j0 += G) {
+  // a single-pass step that feeds the next one: its selected rows stay in shared memory, where
+  // the sources are added and the next x transform runs (no round trip through `out`)
+  const bool fast = npass == 1 && !ps[0].refl && !a.pid && a.xnext;
+  for (int j0 = 0; j0 < npass && !fast; j0 += G) {
     const int g = min(G, npass - j0);  // passes in this group: the transform has 2·rows·g lanes
     // per (pass, x) a run of `rows` pixels (transposed planes); four pixels in flight per thread
     const int npix = g * rows * nx;
@@ -514,6 +518,54 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
       }
     }
     __syncthreads();
+  }
+  if (fast) {
+    for (int idx = tid; idx < rows * nx; idx += nt) {
+      const int row = idx / nx, x = idx - row * nx;
+      cx<T> v0{0, 0}, v1{0, 0};
+      if (row < here)
+        ld_px(a.work + (static_cast<long long>(x) * ny + y0 + row) * 2, v0, v1);
+      buf[(x * rows + row) * 2] = v0;
+      buf[(x * rows + row) * 2 + 1] = v1;
+    }
+    __syncthreads();
+    fft_smem<+1>(buf, plan, tw, 2 * rows, tid, nt);
+    for (int idx = tid; idx < here * nx; idx += nt) {  // scale, mask (and store) in place
+      const int row = idx / nx, x = idx - row * nx;
+      const long long q = static_cast<long long>(y0 + row) * nx + x;
+      const int b = (x * rows + row) * 2;
+      cx<T> v0 = buf[b] * a.inv_n, v1 = buf[b + 1] * a.inv_n;
+      if (a.mask) {
+        v0 = mmul(v0, a.mask, q, n);
+        v1 = mmul(v1, a.mask, q, n);
+      }
+      buf[b] = v0;
+      buf[b + 1] = v1;
+      if (a.store_out && !a.add) st_px(a.out + 2 * q, v0, v1);
+    }
+    __syncthreads();
+    if (a.add) {
+      for (int k = k0 + tid; k < k1; k += nt) {  // interface pixels are distinct
+        const int q = a.iface[k];
+        const int b = ((q - (q / nx) * nx) * rows + (q / nx - y0)) * 2;
+        buf[b] = buf[b] + a.add[2 * k];
+        buf[b + 1] = buf[b + 1] + a.add[2 * k + 1];
+      }
+      __syncthreads();
+      if (a.store_out)
+        for (int idx = tid; idx < here * nx; idx += nt) {
+          const int row = idx / nx, x = idx - row * nx;
+          const int b = (x * rows + row) * 2;
+          st_px(a.out + 2 * (static_cast<long long>(y0 + row) * nx + x), buf[b], buf[b + 1]);
+        }
+    }
+    fft_smem<-1>(buf, plan, tw, 2 * rows, tid, nt);
+    for (int idx = tid; idx < nx * here; idx += nt) {
+      const int x = idx / here, row = idx - x * here;
+      st_px(a.xnext + (static_cast<long long>(x) * ny + y0 + row) * 2, buf[(x * rows + row) * 2],
+            buf[(x * rows + row) * 2 + 1]);
+    }
+    return;
   }
   if (a.add)
     for (int k = k0 + tid; k < k1; k += nt) {

@@ -70,8 +70,10 @@ class PlaneSolver final : public Solver {
   void ensure_passes(bool with_backward);
   // x_ready: xbuf_ already holds the x transform of `in` (3D, fused into the previous step);
   // x_next: also leave the x transform of `out` in xbuf_ for the next step
+  // need_out: the output plane is read after the step (with x_next the next step reads only its
+  // x transform; `out` is still needed for keep planes and a sweep's last plane)
   void step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out, const C* add,
-            bool want_spec, bool x_ready = false, bool x_next = false);
+            bool want_spec, bool x_ready = false, bool x_next = false, bool need_out = true);
   void fft_plane(const C* in, C* out, int ncomp, int dir);
   // out = G·in (combine 0) or in − G·in/2 (combine 1)
   void born_operator(const C* in, C* out, int slot, int dir, int combine = 0);
@@ -682,7 +684,7 @@ void PlaneSolver<T>::ensure_passes(bool with_backward) {
 
 template <typename T>
 void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* out, C* refl_out,
-                          const C* add, bool want_spec, bool x_ready, bool x_next) {
+                          const C* add, bool want_spec, bool x_ready, bool x_next, bool need_out) {
   const StepInfo& st = steps_[s];
   const int dir = backward ? 1 : 0;
   const PassRec* ps = pass_pool_.ptr + pass_off_[dir][s];
@@ -737,6 +739,7 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   r.nx = nx;
   r.rows = sel_.rows;
   r.group = sel_.group;
+  r.store_out = need_out ? 1 : 0;
   r.inv_n = inv_n;
   launch(k_rows_select<T>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, r, ps, npass,
          hx_.plan, tw_x_.ptr);
@@ -959,7 +962,8 @@ void PlaneSolver<T>::sweeps(int iterations, const std::vector<int>& keep_slot, D
       // touches the plane between two steps of a sweep)
       const bool fuse = !is2d() && !born;
       step(p, false, reflect, e, next, reflect ? src_bwd_.ptr + 2 * st.iface_off : nullptr, add, host,
-           fuse && p > 0, fuse && p + 1 < nz);
+           fuse && p > 0, fuse && p + 1 < nz,
+           !(fuse && p + 1 < nz) || (last && keep_slot[p + 1] >= 0));
       if (host) {
         born_step(spec_.ptr, inc_.ptr, st.host_slot, +1);
         add_plane_scaled(next, inc_.ptr, mask_.ptr);
@@ -991,7 +995,7 @@ void PlaneSolver<T>::sweeps(int iterations, const std::vector<int>& keep_slot, D
       const C* add = st.niface > 0 ? src_bwd_.ptr + 2 * st.iface_off : nullptr;
       const bool fuse = !is2d() && !born;
       step(p - 1, true, reflect, e, next, reflect ? src_fwd_.ptr + 2 * st.iface_off : nullptr, add, false,
-           fuse && p < nz, fuse && p > 1);
+           fuse && p < nz, fuse && p > 1, !(fuse && p > 1) || (last && keep_slot[p - 1] >= 0));
       std::swap(e, next);
       if (born && p >= 2 && steps_[p - 2].host_slot >= 0)
         add_plane_scaled(e, born_bwd_.ptr + steps_[p - 2].host_slot * n2, nullptr);  // born_bwd[p − 1]
