@@ -196,8 +196,9 @@ __device__ __forceinline__ void dft(cx<T>* u) {
 // One stage of radix R on `batch` lanes (point stride `batch`), in place; a thread stages up to
 // EPT values (kmax_for(R, EPT) butterflies).
 template <int DIR, int R, int EPT, typename T>
-__device__ __noinline__ void stage(cx<T>* buf, int n, int len, const Tw<T>* __restrict__ tw,
-                                      int batch, int tid, int nthreads) {
+__device__ __forceinline__ void stage_body(cx<T>* buf, int n, int len,
+                                           const Tw<T>* __restrict__ tw, int batch, int tid,
+                                           int nthreads) {
   constexpr int K = kmax_for(R, EPT);
   const int nb = n / R;
   const int total = nb * batch;
@@ -229,6 +230,12 @@ __device__ __noinline__ void stage(cx<T>* buf, int n, int len, const Tw<T>* __re
       for (int r = 0; r < R; ++r) buf[dst[k] + r * len * batch] = u[k][r];
     }
   __syncthreads();
+}
+
+template <int DIR, int R, int EPT, typename T>
+__device__ __noinline__ void stage(cx<T>* buf, int n, int len, const Tw<T>* __restrict__ tw,
+                                   int batch, int tid, int nthreads) {
+  stage_body<DIR, R, EPT>(buf, n, len, tw, batch, tid, nthreads);
 }
 
 // Generic odd radix R ≤ kMaxGenericRadix by the symmetric real-cosine form; one butterfly
@@ -285,6 +292,31 @@ __device__ __noinline__ void fft_smem(cx<T>* buf, const FftPlan& plan, const Tw<
       case 5: stage<DIR, 5, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
       case 7: stage<DIR, 7, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
       case 8: stage<DIR, 8, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
+      default:
+        stage_generic<DIR>(buf, plan.n, len, r, w, tw + plan.rootoff, batch, tid, nthreads);
+    }
+  }
+}
+
+// The same transform with the radix 2-8 stages expanded in the caller. A call of a stage
+// function saves and restores the caller's live registers through local memory at every stage;
+// the 3D plane kernels, whose threads hold pixel data and table values across their
+// transforms, use this form. The generic radix stays a call.
+template <int DIR, int EPT = 16, typename T>
+__device__ __forceinline__ void fft_smem_inline(cx<T>* buf, const FftPlan& plan,
+                                                const Tw<T>* __restrict__ tw, int batch, int tid,
+                                                int nthreads) {
+  using namespace fftdetail;
+  for (int s = 0; s < plan.nstages; ++s) {
+    const int r = plan.radix[s], len = plan.len[s];
+    const Tw<T>* w = tw + plan.twoff[s];
+    switch (r) {
+      case 2: stage_body<DIR, 2, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
+      case 3: stage_body<DIR, 3, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
+      case 4: stage_body<DIR, 4, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
+      case 5: stage_body<DIR, 5, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
+      case 7: stage_body<DIR, 7, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
+      case 8: stage_body<DIR, 8, EPT>(buf, plan.n, len, w, batch, tid, nthreads); break;
       default:
         stage_generic<DIR>(buf, plan.n, len, r, w, tw + plan.rootoff, batch, tid, nthreads);
     }

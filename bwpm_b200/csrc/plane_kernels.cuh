@@ -23,6 +23,12 @@ namespace bwpm {
 
 constexpr int kMaxPasses = 128;
 constexpr int kPlaneThreads = 512;  // CTA width limit of the plane kernels (128 registers)
+// Register budget of the 3D step kernels, as CTAs of kPlaneThreads per SM: complex64 runs
+// faster with two (64 registers, some spills, twice the warps), FP64 with one (128 registers;
+// its butterflies hold twice the bytes). Measured per slab pass on the 512² microlens:
+// complex64 64.3 µs (two) against 73.4 µs (one), FP64 115.8 against 99.1 µs.
+template <typename T>
+constexpr int kPlaneMinBlocks = sizeof(T) == sizeof(double) ? 1 : 2;
 
 // Table entry times field value. FP64 tables hold one value per entry; FP32 tables hold the
 // FP64 value as hi + lo with the lo block `lo` entries after the hi block (see fft.cuh on why
@@ -144,8 +150,8 @@ __global__ void __launch_bounds__(kPlaneThreads) k_step2d(Step2D<T> a, const Pas
 // TOUT: the output is stored transposed, out[(x·ny + y)·ncomp + c] (the layout the column
 // kernel of a slab step reads contiguously); otherwise row-major like the input.
 template <int DIR, typename T, bool TOUT = false>
-__global__ void __launch_bounds__(kPlaneThreads) k_rows_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int rows,
-                           FftPlan plan, const Tw<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks<T>) k_rows_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int rows,
+                           const __grid_constant__ FftPlan plan, const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int y0 = blockIdx.x * rows;
@@ -160,7 +166,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_fft(const cx<T>* in, cx<
         row < here ? in[(static_cast<long long>(y0 + row) * nx + x) * ncomp + c] : cx<T>{0, 0};
   }
   __syncthreads();
-  fft_smem<DIR>(buf, plan, tw, rows * ncomp, tid, nt);
+  fft_smem_inline<DIR>(buf, plan, tw, rows * ncomp, tid, nt);
   if constexpr (TOUT) {  // per x a run of `here` rows × ncomp, contiguous in both memories
     const int run = here * ncomp;
     for (int idx = tid; idx < nx * run; idx += nt) {
@@ -190,7 +196,7 @@ struct ColStep {
 // 3D solve are stored transposed (x-major), so every column is one contiguous run in memory.
 // smem: spectrum tile [y][col][2] and, for several passes, a work tile.
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const PassRec* __restrict__ ps, int npass, FftPlan plan,
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks<T>) k_cols_step(ColStep<T> a, const PassRec* __restrict__ ps, int npass, const __grid_constant__ FftPlan plan,
                             const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* sbuf = reinterpret_cast<cx<T>*>(smem_raw);
@@ -208,7 +214,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
         x < nx ? a.in[static_cast<long long>(x) * run + rem] : cx<T>{0, 0};
   }
   __syncthreads();
-  fft_smem<-1>(sbuf, plan, tw, 2 * cols, tid, nt);
+  fft_smem_inline<-1>(sbuf, plan, tw, 2 * cols, tid, nt);
   if (a.spec_out)
     for (int idx = tid; idx < tile; idx += nt) {
       const int y = idx / (2 * cols), rem = idx - y * 2 * cols;
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
           }
         }
         __syncthreads();
-        fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
+        fft_smem_inline<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
         cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
         for (int idx = tid; idx < tile; idx += nt) {
           const int xc = idx / run, rem = idx - xc * run;
@@ -291,7 +297,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
       }
     }
     __syncthreads();
-    fft_smem<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
+    fft_smem_inline<+1>(wbuf, plan, tw, 2 * cols, tid, nt);
     cx<T>* w = a.work + static_cast<long long>(j) * 2 * n;
     for (int idx = tid; idx < tile; idx += nt) {
       const int xc = idx / run, rem = idx - xc * run;
@@ -310,8 +316,8 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step(ColStep<T> a, const
 // (16-byte runs) and 16-byte aligned planes (the host checks).
 // smem: column [y][c] (2·ny), work tile (2·G·ny), one mbarrier.
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, const PassRec* __restrict__ ps, int npass,
-                                 FftPlan plan, const Tw<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks<T>) k_cols_step_bulk(ColStep<T> a, const PassRec* __restrict__ ps, int npass,
+                                 const __grid_constant__ FftPlan plan, const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kB = table_blocks<T>();
   constexpr int U = 4;  // points per thread whose table values load together
@@ -332,7 +338,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
     bulk_load(sbuf, a.in + static_cast<long long>(x) * 2 * ny, run_bytes, mbar);
   }
   bulk_wait(mbar, 0, a.status);
-  fft_smem<-1>(sbuf, plan, tw, 2, tid, nt);
+  fft_smem_inline<-1>(sbuf, plan, tw, 2, tid, nt);
   if (a.spec_out)
     for (int i = tid; i < 2 * ny; i += nt)
       a.spec_out[(static_cast<long long>(i >> 1) * a.nx + x) * 2 + (i & 1)] = sbuf[i];
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_step_bulk(ColStep<T> a, 
       }
     }
     __syncthreads();
-    fft_smem<+1>(wbuf, plan, tw, 2 * g, tid, nt);
+    fft_smem_inline<+1>(wbuf, plan, tw, 2 * g, tid, nt);
     for (int idx = tid; idx < g * ny; idx += nt) {  // per pass one contiguous column, by pixel
       const int gi = idx / ny, y = idx - gi * ny;
       st_px(a.work + static_cast<long long>(j0 + gi) * 2 * n + (static_cast<long long>(x) * ny + y) * 2,
@@ -444,7 +450,7 @@ struct RowSelect {
 
 // inverse x transform of each pass for `rows` rows, then select/mask/gather/add.
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, const PassRec* __restrict__ ps, int npass, FftPlan plan,
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks<T>) k_rows_select(RowSelect<T> a, const PassRec* __restrict__ ps, int npass, const __grid_constant__ FftPlan plan,
                               const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
@@ -489,7 +495,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
         }
     }
     __syncthreads();
-    fft_smem<+1>(buf, plan, tw, 2 * rows * g, tid, nt);
+    fft_smem_inline<+1>(buf, plan, tw, 2 * rows * g, tid, nt);
     for (int gi = 0; gi < g; ++gi) {
       const int j = j0 + gi;
       const int pair = ps[j].pair;
@@ -529,7 +535,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
       buf[(x * rows + row) * 2 + 1] = v1;
     }
     __syncthreads();
-    fft_smem<+1>(buf, plan, tw, 2 * rows, tid, nt);
+    fft_smem_inline<+1>(buf, plan, tw, 2 * rows, tid, nt);
     for (int idx = tid; idx < here * nx; idx += nt) {  // scale, mask (and store) in place
       const int row = idx / nx, x = idx - row * nx;
       const long long q = static_cast<long long>(y0 + row) * nx + x;
@@ -559,7 +565,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
           st_px(a.out + 2 * (static_cast<long long>(y0 + row) * nx + x), buf[b], buf[b + 1]);
         }
     }
-    fft_smem<-1>(buf, plan, tw, 2 * rows, tid, nt);
+    fft_smem_inline<-1>(buf, plan, tw, 2 * rows, tid, nt);
     for (int idx = tid; idx < nx * here; idx += nt) {
       const int x = idx / here, row = idx - x * here;
       st_px(a.xnext + (static_cast<long long>(x) * ny + y0 + row) * 2, buf[(x * rows + row) * 2],
@@ -583,7 +589,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_rows_select(RowSelect<T> a, c
       buf[(x * rows + row) * 2 + 1] = v1;
     }
     __syncthreads();
-    fft_smem<-1>(buf, plan, tw, 2 * rows, tid, nt);
+    fft_smem_inline<-1>(buf, plan, tw, 2 * rows, tid, nt);
     for (int idx = tid; idx < nx * here; idx += nt) {  // transposed: per x a run of `here` pixels
       const int x = idx / here, row = idx - x * here;
       st_px(a.xnext + (static_cast<long long>(x) * ny + y0 + row) * 2, buf[(x * rows + row) * 2],
