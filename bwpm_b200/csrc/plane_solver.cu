@@ -24,6 +24,7 @@
 #include "gmres_kernels.cuh"
 #include "plan.hpp"
 #include "plane_kernels.cuh"
+#include "plane_rf.cuh"
 #include "plane_setup.cuh"
 #include "solver.hpp"
 
@@ -134,6 +135,9 @@ class PlaneSolver final : public Solver {
   int sms_ = 148;
   LaunchShape rows2_, rows3_, sel_, cols1_, cols2_, cols3_;
   std::int64_t launches_ = 0, gmres_applies_ = 0;
+  // complex64 3D: the fixed-length step kernels (plane_rf.cuh) when both lateral sizes have one
+  RfKernels rf_y_, rf_x_;
+  DevBuf<Tw<float>> tw_rf_y_, tw_rf_x_;
   bool cols_bulk_ = false;  // 3D column kernel with bulk copies (k_cols_step_bulk)
   int cols_bulk_threads_ = 256, cols_bulk_group_ = 1;
   DevBuf<int> status_;      // set by a kernel whose bounded wait gave up
@@ -486,6 +490,29 @@ void PlaneSolver<T>::setup() {
                    (const void*)k_rows_select<T>,
                    (const void*)k_cols_fft<-1, T>, (const void*)k_cols_fft<1, T>})
       check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+    // complex64: fixed-length kernels where ny and nx have them (whole CTAs of lines);
+    // BWPM_3D_KERNELS=general selects the general kernels
+    const char* kk = std::getenv("BWPM_3D_KERNELS");
+    if (sizeof(T) == sizeof(float) && !(kk && std::strcmp(kk, "general") == 0)) {
+      RfKernels ky = rf_kernels(nyi), kx = rf_kernels(static_cast<int>(in_.nx));
+      if (ky.cols && kx.rows && in_.nx % ky.lines == 0 && in_.ny % kx.lines == 0) {
+        rf_y_ = ky;
+        rf_x_ = kx;
+        auto upload_rf = [&](const RfKernels& k, int len, DevBuf<Tw<float>>& d) {
+          const std::vector<Tw<float>> t = twiddles_for<float>(make_plan_radices(len, k.radices));
+          d.alloc(t.size(), stream_);
+          d.upload(t.data(), t.size());
+        };
+        upload_rf(rf_y_, nyi, tw_rf_y_);
+        upload_rf(rf_x_, static_cast<int>(in_.nx), tw_rf_x_);
+        check_cuda(cudaFuncSetAttribute((const void*)rf_y_.cols,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(rf_y_.smem)), "smem");
+        check_cuda(cudaFuncSetAttribute((const void*)rf_x_.rows,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(rf_x_.smem)), "smem");
+      }
+    }
   }
   // operator tables of the forward transmission (all runs need them)
   for (std::size_t p = 0; p < in_.nz; ++p)
@@ -714,6 +741,33 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
   if (!x_ready)  // the x transform of the step's input, stored transposed for the column kernel
     launch(k_rows_fft<-1, T, true>, dim3(ceil_div(ny, sel_.rows)), dim3(sel_.threads), sel_.smem, in,
            xbuf_.ptr, ny, nx, 2, sel_.rows, hx_.plan, tw_x_.ptr);
+  if constexpr (sizeof(T) == sizeof(float)) {
+    if (rf_y_.cols) {
+      ColStep<float> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, 0,
+                       status_.ptr};
+      launch(rf_y_.cols, dim3(nx / rf_y_.lines), dim3(kRfThreads), rf_y_.smem, c, ps, npass,
+             (const Tw<float>*)tw_rf_y_.ptr);
+      RowSelect<float> r;
+      r.work = work_.ptr;
+      r.out = out;
+      r.pid = pid;
+      r.mask = mask_.ptr;
+      r.iface = iface;
+      r.rowoff = st.rowoff_off >= 0 ? rowoff_pool_.ptr + st.rowoff_off : nullptr;
+      r.refl_out = refl_out;
+      r.add = add;
+      r.xnext = x_next ? xbuf_.ptr : nullptr;
+      r.ny = ny;
+      r.nx = nx;
+      r.rows = rf_x_.lines;
+      r.group = 1;
+      r.store_out = need_out ? 1 : 0;
+      r.inv_n = inv_n;
+      launch(rf_x_.rows, dim3(ny / rf_x_.lines), dim3(kRfThreads), rf_x_.smem, r, ps, npass,
+             (const Tw<float>*)tw_rf_x_.ptr);
+      return;
+    }
+  }
   if (cols_bulk_) {
     ColStep<T> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, cols_bulk_group_,
                  status_.ptr};

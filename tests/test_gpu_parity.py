@@ -231,6 +231,7 @@ def test_bulk_column_kernel_equals_plain_loads(core, monkeypatch, prefix, iters,
     out = {}
     for mode in ("plain", "bulk"):
         monkeypatch.setenv("BWPM_COLS", mode)
+        monkeypatch.setenv("BWPM_3D_KERNELS", "general")
         out[mode] = core.CudaSolver(*args, 0, fluctuation=fl, precision=precision).run(
             field, iters, [0, 5])
     a, b = out["plain"], out["bulk"]
