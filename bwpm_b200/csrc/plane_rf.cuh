@@ -210,7 +210,10 @@ __global__ void __launch_bounds__(kRfThreads, 2)
 // selection by pair id, mask and reflection gather; then the sparse sources, the output rows and
 // (with xnext) their forward x transform, stored x-major (k_rows_select's contract; a.rows,
 // a.group unused). Every pixel belongs to exactly one transmission pass (its pair's). The host
-// launches ny / lines CTAs (ny a multiple of the lines).
+// launches ny / lines CTAs (ny a multiple of the lines). The lines of a CTA interleave within a
+// warp (line = thread mod lines), so one warp access covers the whole x-major run of the CTA's
+// rows at each of its x (whole 32-byte sectors): with one line per warp, every sector was
+// requested by as many warps as lines (512² microlens: 43.0 → 36.9 µs per slab pass).
 template <int NX>
 __global__ void __launch_bounds__(kRfThreads, 2)
     k_rows_rf(RowSelect<float> a, const PassRec* __restrict__ ps, int npass,
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(kRfThreads, 2)
   constexpr int NT = PlaneRf<NX>::NT, E = NX / NT, P = rf::padded(NX), LN = rf_lines<NX>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cf* sm = reinterpret_cast<cf*>(smem_raw);
-  const int line = threadIdx.x / NT, t = threadIdx.x % NT;
+  const int line = threadIdx.x % LN, t = threadIdx.x / LN;
   cf* base = sm + static_cast<long long>(line) * 4 * P;
   cf* const buf[2][2] = {{base, base + P}, {base + 2 * P, base + 3 * P}};
   const int ny = a.ny;
