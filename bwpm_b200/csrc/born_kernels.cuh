@@ -51,13 +51,26 @@ __global__ void k_born_half(const cx<T>* in, cx<T>* out, BornGrid g, double sign
   out[2 * q + 1] = cast<T>(cast<double>(in[2 * q + 1]) * f);
 }
 
+// The Born slab of the current step in device memory (grid with the slab's host index,
+// direction, potential plane): the operator kernels of the GMRES cycle graph, captured once per
+// solver, read it here, so one graph serves every slab and both directions.
+template <typename T>
+struct BornCur {
+  BornGrid g;
+  int dir;
+  const cx<T>* pot;
+};
+
+template <typename T>
+__global__ void k_set_born_cur(BornCur<T>* cur, BornCur<T> v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *cur = v;
+}
+
 // w3 = (Ŝ_x, Ŝ_y, −d·k⊥·Ŝ⊥/k_z)·e^{i k_z s} on propagating waves (s = 0: no phase), 0 elsewhere.
 template <typename T>
-__global__ void k_born_prepare(const cx<T>* spec, cx<T>* w3, BornGrid g, int direction,
-                               double distance) {
-  const long long n = static_cast<long long>(g.ny) * g.nx;
-  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (q >= n) return;
+__device__ __forceinline__ void born_prepare_at(long long q, const cx<T>* spec, cx<T>* w3,
+                                                const BornGrid& g, int direction,
+                                                double distance) {
   const BornPoint p = born_point(g, q);
   if (!p.prop) {
     w3[3 * q] = w3[3 * q + 1] = w3[3 * q + 2] = cx<T>{0, 0};
@@ -72,6 +85,22 @@ __global__ void k_born_prepare(const cx<T>* spec, cx<T>* w3, BornGrid g, int dir
   w3[3 * q + 2] = cast<T>(ez * ph);
 }
 
+template <typename T>
+__global__ void k_born_prepare(const cx<T>* spec, cx<T>* w3, BornGrid g, int direction,
+                               double distance) {
+  const long long n = static_cast<long long>(g.ny) * g.nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q < n) born_prepare_at(q, spec, w3, g, direction, distance);
+}
+
+template <typename T>
+__global__ void k_born_prepare_cur(const cx<T>* spec, cx<T>* w3, const BornCur<T>* cur) {
+  const BornGrid g = cur->g;
+  const long long n = static_cast<long long>(g.ny) * g.nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q < n) born_prepare_at(q, spec, w3, g, cur->dir, 0.0);
+}
+
 // w3 *= V·(1/N) in real space, V = 2ñ₀k₀²δn precomputed per pixel.
 template <typename T>
 __global__ void k_born_potential(cx<T>* w3, const cx<T>* v, long long n, T inv_n) {
@@ -81,12 +110,18 @@ __global__ void k_born_potential(cx<T>* w3, const cx<T>* v, long long n, T inv_n
   for (int c = 0; c < 3; ++c) w3[3 * q + c] = s * w3[3 * q + c];
 }
 
-// out = i dz/(2k_z)·(Ŝ⊥ − k⊥·(k⊥·Ŝ⊥ + d·k_z·Ŝ_z)/k²) on propagating waves, 0 elsewhere.
 template <typename T>
-__global__ void k_born_finish(const cx<T>* w3, cx<T>* out, BornGrid g, int direction) {
-  const long long n = static_cast<long long>(g.ny) * g.nx;
+__global__ void k_born_potential_cur(cx<T>* w3, const BornCur<T>* cur, long long n, T inv_n) {
   const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (q >= n) return;
+  const cx<T> s = cur->pot[q] * inv_n;
+  for (int c = 0; c < 3; ++c) w3[3 * q + c] = s * w3[3 * q + c];
+}
+
+// out = i dz/(2k_z)·(Ŝ⊥ − k⊥·(k⊥·Ŝ⊥ + d·k_z·Ŝ_z)/k²) on propagating waves, 0 elsewhere.
+template <typename T>
+__device__ __forceinline__ void born_finish_at(long long q, const cx<T>* w3, cx<T>* out,
+                                               const BornGrid& g, int direction) {
   const BornPoint p = born_point(g, q);
   if (!p.prop) {
     out[2 * q] = out[2 * q + 1] = cx<T>{0, 0};
@@ -100,6 +135,21 @@ __global__ void k_born_finish(const cx<T>* w3, cx<T>* out, BornGrid g, int direc
   const cd lon = cdiv(p.kx * s0 + p.ky * s1 + (static_cast<double>(direction) * p.kz) * s2, k2);
   out[2 * q] = cast<T>(green * (s0 - p.kx * lon));
   out[2 * q + 1] = cast<T>(green * (s1 - p.ky * lon));
+}
+
+template <typename T>
+__global__ void k_born_finish(const cx<T>* w3, cx<T>* out, BornGrid g, int direction) {
+  const long long n = static_cast<long long>(g.ny) * g.nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q < n) born_finish_at(q, w3, out, g, direction);
+}
+
+template <typename T>
+__global__ void k_born_finish_cur(const cx<T>* w3, cx<T>* out, const BornCur<T>* cur) {
+  const BornGrid g = cur->g;
+  const long long n = static_cast<long long>(g.ny) * g.nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q < n) born_finish_at(q, w3, out, g, cur->dir);
 }
 
 // total = Σ_m ½·e^{i d′k_z(1−ζ_m)dz}·i dz/(2k_z)·[P(k_d′)·Ŝ_m]⊥ (spectrum), sources (2, N, 3).

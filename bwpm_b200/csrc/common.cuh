@@ -112,9 +112,14 @@ struct invalid_argument : std::invalid_argument {
   using std::invalid_argument::invalid_argument;
 };
 
+// Throws on a failed runtime call. The runtime also keeps a failed call's code as its "last
+// error", which the next launch check (cudaGetLastError) would report against an unrelated
+// kernel: it is read (and so cleared, unless the context itself is lost) before throwing.
 inline void check_cuda(cudaError_t e, const char* what) {
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
     throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 
 inline unsigned ceil_div(std::size_t a, std::size_t b) { return static_cast<unsigned>((a + b - 1) / b); }

@@ -81,8 +81,6 @@ struct DevBuf {
   }
 };
 
-// A non-blocking stream owned by a solver; declared before the solver's buffers so that it is
-// destroyed after them.
 // RAII page-locked host allocation (cudaHostAlloc).
 template <typename U>
 struct PinnedBuf {
@@ -121,6 +119,21 @@ struct OwnedEvent {
   operator cudaEvent_t() const { return e; }
 };
 
+// RAII CUDA graph and its executable form.
+struct OwnedGraph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  OwnedGraph() = default;
+  ~OwnedGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g) cudaGraphDestroy(g);
+  }
+  OwnedGraph(const OwnedGraph&) = delete;
+  OwnedGraph& operator=(const OwnedGraph&) = delete;
+};
+
+// A non-blocking stream owned by a solver; declared before the solver's buffers so that it is
+// destroyed after them.
 struct OwnedStream {
   cudaStream_t s = nullptr;
   OwnedStream() = default;

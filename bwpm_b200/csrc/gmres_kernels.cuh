@@ -7,9 +7,10 @@
 // inner products, the Hessenberg matrix, the rotations and the solution of the small triangular
 // system stay in device memory: the dot kernels write h straight into the Hessenberg matrix, the
 // vector updates read their coefficients from it, and one thread applies the rotations. The host
-// learns of convergence through a flag copied to pinned memory, one Arnoldi step behind (the
-// step after a converged one is computed speculatively and discarded: it touches no entry the
-// solution uses).
+// learns of convergence from the flags: by default once per restart cycle, which runs as a CUDA
+// graph whose Arnoldi steps sit under conditional nodes that the rotation kernel clears on
+// convergence; or (host-driven form) one Arnoldi step behind, the step after a converged one
+// computed speculatively and discarded (it touches no entry the solution uses).
 #pragma once
 
 #include "common.cuh"
@@ -27,6 +28,7 @@ struct GmresState {
   cd dot;        // scratch inner product (norms)
   double nrm;    // last norm
   double hnext[kGmresRestart];
+  double tolb;   // tolerance × ‖rhs‖ of the current solve (read by the cycle graph)
   int flag[kGmresRestart];
   unsigned counter;  // last-block ticket of the dot kernels (back at 0 after each dot)
 };
@@ -87,16 +89,17 @@ __global__ void k_norm_scale(cx<T>* out, const cx<T>* in, const cd* dot, double*
   out[i] = cast<T>(cd{0.0, 0.0} + cast<double>(in[i]) * inv);
 }
 
-// g = (β, 0, …, 0) with β = √Re(dot).
-__global__ void k_gmres_start(GmresState* s) {
+// g = (β, 0, …, 0) with β = √Re(dot); the cycle's flags cleared; tolb = tol·‖rhs‖.
+__global__ void k_gmres_start(GmresState* s, double tol_bnorm) {
   const int i = threadIdx.x;
   if (i <= kGmresRestart) s->g[i] = cd{i == 0 ? sqrt(s->dot.re) : 0.0, 0.0};
+  if (i < kGmresRestart) s->flag[i] = 0;
+  if (i == 0) s->tolb = tol_bnorm;
 }
 
 // Column j of the Arnoldi step: earlier rotations, the new rotation from h[j][j] and
 // hnext = √Re(dot) (cpp/src/solver.cpp:164-190); flag[j] = converged or breakdown.
-__global__ void k_gmres_givens(GmresState* s, int j, double tol_bnorm) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void gmres_givens(GmresState* s, int j, double tol_bnorm) {
   constexpr int m = kGmresRestart;
   const double hnext = sqrt(s->dot.re);
   s->hnext[j] = hnext;
@@ -119,6 +122,21 @@ __global__ void k_gmres_givens(GmresState* s, int j, double tol_bnorm) {
   s->g[j + 1] = -(conj(s->sn[j]) * s->g[j]);
   s->g[j] = s->cs[j] * s->g[j];
   s->flag[j] = (hypot(s->g[j + 1].re, s->g[j + 1].im) <= tol_bnorm || hnext == 0.0) ? 1 : 0;
+}
+
+__global__ void k_gmres_givens(GmresState* s, int j, double tol_bnorm) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  gmres_givens(s, j, tol_bnorm);
+}
+
+// The same as the last node of Arnoldi step j in the cycle graph: the tolerance comes from the
+// state, and the condition of step j + 1's node (`next`, when there is one) is set unless step j
+// has converged.
+__global__ void k_gmres_givens_cond(GmresState* s, int j, cudaGraphConditionalHandle next,
+                                    int has_next) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  gmres_givens(s, j, s->tolb);
+  if (has_next) cudaGraphSetConditional(next, s->flag[j] ? 0u : 1u);
 }
 
 // Back substitution for the first `used` unknowns (cpp/src/solver.cpp:193-199).

@@ -77,11 +77,13 @@ class PlaneSolver final : public Solver {
             bool want_spec, bool x_ready = false, bool x_next = false, bool need_out = true);
   void fft_plane(const C* in, C* out, int ncomp, int dir);
   // out = G·in (combine 0) or in − G·in/2 (combine 1)
-  void born_operator(const C* in, C* out, int slot, int dir, int combine = 0);
+  void born_operator(const C* in, C* out, int combine = 0);
   void born_step(const C* spec, C* inc, int slot, int dir);
   void born_sources(const C* spec, int slot, int dir);
   void born_emission(int slot, int dir, C* plane);
-  void gmres(int slot, int dir);
+  void gmres();
+  void arnoldi_step(int j, bool in_graph, double tol_bnorm);
+  void build_cycle_graph();
   // the forward/backward sweeps of a run (device work only, unless Born slabs need GMRES)
   void sweeps(int iterations, const std::vector<int>& keep_slot, DevBuf<C>& kept_f, DevBuf<C>& kept_b,
               DevBuf<C>& t_iter, DevBuf<C>& r_iter);
@@ -127,6 +129,10 @@ class PlaneSolver final : public Solver {
       g_tmp2_, inc_;
   std::vector<DevBuf<C>> basis_;
   DevBuf<GmresState> gst_;
+  DevBuf<BornCur<T>> born_cur_;  // the Born slab of the current step (set per step)
+  OwnedGraph cycle_;             // one GMRES restart cycle (Arnoldi steps under conditionals)
+  cudaGraphConditionalHandle cycle_cond_[kGmresRestart] = {};  // one per step's node
+  int gm_vblocks_ = 0, gm_dblocks_ = 0;
   DevBuf<cd> dot_partial_;
   PinnedBuf<int> flags_host_;
   OwnedEvent gmres_events_[kGmresRestart];
@@ -523,6 +529,7 @@ void PlaneSolver<T>::setup() {
     }
   // Born: potential V = 2ñ₀k₀²δn per host slab, full-plane source stores
   if (!hosts_.empty()) {
+    born_cur_.alloc(1, stream_);
     pot_.alloc(hosts_.size() * nn, stream_);
     std::vector<C> vt(hosts_.size() * nn);
     for (std::size_t p = 0; p < in_.nz; ++p) {
@@ -828,17 +835,17 @@ void PlaneSolver<T>::fft_plane(const C* in, C* out, int ncomp, int dir) {
 }
 
 template <typename T>
-void PlaneSolver<T>::born_operator(const C* in, C* out, int slot, int dir, int combine) {
-  // cpp/src/solver.cpp:262-311
-  const BornGrid g = born_grid(slot);
+void PlaneSolver<T>::born_operator(const C* in, C* out, int combine) {
+  // cpp/src/solver.cpp:262-311, for the slab in born_cur_ (set by born_step)
   const long long nn = static_cast<long long>(n());
-  launch(k_born_prepare<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, in, w3_.ptr, g, dir, 0.0);
+  const BornCur<T>* cur = born_cur_.ptr;
+  launch(k_born_prepare_cur<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, in, w3_.ptr, cur);
   fft_plane(w3_.ptr, w3_.ptr, 3, +1);
-  launch(k_born_potential<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr,
-         (const C*)(pot_.ptr + slot * nn), nn, static_cast<T>(1.0 / static_cast<double>(nn)));
+  launch(k_born_potential_cur<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr, cur,
+         nn, static_cast<T>(1.0 / static_cast<double>(nn)));
   fft_plane(w3_.ptr, w3_.ptr, 3, -1);
-  launch(k_born_finish<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, (const C*)w3_.ptr, out,
-         g, dir);
+  launch(k_born_finish_cur<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0,
+         (const C*)w3_.ptr, out, cur);
   if (combine) {  // out = in − G·in/2
     check_cuda(cudaMemcpyAsync(g_tmp2_.ptr, out, 2 * nn * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
     check_cuda(cudaMemcpyAsync(out, in, 2 * nn * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
@@ -859,12 +866,80 @@ void PlaneSolver<T>::add_plane_scaled(C* dst, const C* src, const T* mask) {
          static_cast<T>(1.0 / static_cast<double>(n())), n2);
 }
 
-// GMRES(30) for (1 − G/2)·y = rhs with start y = rhs (cpp/src/solver.cpp:130-207, :336-342),
-// scalar work on the device (gmres_kernels.cuh). The host waits on the device three times per
-// restart (‖rhs‖ once per solve, β, the final residual) and otherwise only for the convergence
-// flag of the previous Arnoldi step while the next one runs.
+// Arnoldi step j of GMRES(30) (modified Gram-Schmidt, cpp/src/solver.cpp:150-190): w = A·v_j,
+// h[i][j] = ⟨v_i, w⟩ and w −= h[i][j]·v_i for i ≤ j, v_{j+1} = w/‖w‖, the rotations. In the cycle
+// graph the rotation kernel also sets the graph's condition for step j + 1; host-driven, the
+// flag goes to pinned memory behind an event.
 template <typename T>
-void PlaneSolver<T>::gmres(int slot, int dir) {
+void PlaneSolver<T>::arnoldi_step(int j, bool in_graph, double tol_bnorm) {
+  constexpr int m = kGmresRestart;
+  const long long m2 = 2 * static_cast<long long>(n());
+  GmresState* st = gst_.ptr;
+  born_operator(basis_[j].ptr, g_w_.ptr, 1);  // w = v_j − G v_j/2
+  for (int i = 0; i <= j; ++i) {
+    launch(k_dot_dev<T>, dim3(gm_dblocks_), dim3(256), 0, (const C*)basis_[i].ptr,
+           (const C*)g_w_.ptr, m2, dot_partial_.ptr, &st->counter, &st->h[i * m + j]);
+    launch(k_axpy_dev<T>, dim3(gm_vblocks_), dim3(kThreads), 0, g_w_.ptr, (const C*)basis_[i].ptr,
+           (const cd*)&st->h[i * m + j], -1.0, m2);
+  }
+  launch(k_dot_dev<T>, dim3(gm_dblocks_), dim3(256), 0, (const C*)g_w_.ptr, (const C*)g_w_.ptr,
+         m2, dot_partial_.ptr, &st->counter, &st->dot);
+  launch(k_norm_scale<T>, dim3(gm_vblocks_), dim3(kThreads), 0, basis_[j + 1].ptr,
+         (const C*)g_w_.ptr, (const cd*)&st->dot, &st->nrm, m2);
+  if (in_graph) {
+    const bool has_next = j + 1 < kGmresRestart;
+    launch(k_gmres_givens_cond, dim3(1), dim3(32), 0, st, j,
+           has_next ? cycle_cond_[j + 1] : cudaGraphConditionalHandle{0}, has_next ? 1 : 0);
+  } else {
+    launch(k_gmres_givens, dim3(1), dim3(32), 0, st, j, tol_bnorm);
+    check_cuda(cudaMemcpyAsync(flags_host_.ptr + j, &st->flag[j], sizeof(int), cudaMemcpyDeviceToHost,
+                               stream_), "flag");
+    check_cuda(cudaEventRecord(gmres_events_[j], stream_), "event");
+  }
+}
+
+// The restart cycle as one graph, built once per solver (the buffers it names are fixed; the
+// slab comes from born_cur_, the tolerance from the state): Arnoldi step j runs under an IF node
+// with a handle of its own (a handle serves one node). Step 0's condition is 1 at each launch,
+// the others 0 until step j − 1 sets them, which it does unless it converged; a skipped step sets
+// nothing, so every later step is skipped too.
+template <typename T>
+void PlaneSolver<T>::build_cycle_graph() {
+  if (cycle_.exec) return;
+  const std::int64_t launches = launches_;
+  check_cuda(cudaGraphCreate(&cycle_.g, 0), "graph create");
+  for (int j = 0; j < kGmresRestart; ++j)
+    check_cuda(cudaGraphConditionalHandleCreate(&cycle_cond_[j], cycle_.g, j == 0 ? 1u : 0u,
+                                                cudaGraphCondAssignDefault),
+               "conditional handle");
+  cudaGraphNode_t prev = nullptr;
+  for (int j = 0; j < kGmresRestart; ++j) {
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = cycle_cond_[j];
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    check_cuda(cudaGraphAddNode(&node, cycle_.g, prev ? &prev : nullptr, prev ? 1 : 0, &p),
+               "conditional node");
+    check_cuda(cudaStreamBeginCaptureToGraph(stream_, p.conditional.phGraph_out[0], nullptr,
+                                             nullptr, 0, cudaStreamCaptureModeThreadLocal),
+               "capture");
+    arnoldi_step(j, true, 0.0);
+    cudaGraph_t body;
+    check_cuda(cudaStreamEndCapture(stream_, &body), "capture");
+    prev = node;
+  }
+  check_cuda(cudaGraphInstantiate(&cycle_.exec, cycle_.g, 0), "instantiate");
+  launches_ = launches;
+}
+
+// GMRES(30) for (1 − G/2)·y = rhs with start y = rhs (cpp/src/solver.cpp:130-207, :336-342),
+// scalar work on the device (gmres_kernels.cuh). The host waits on the device for ‖rhs‖ once per
+// solve and per restart for β, the cycle's flags and the final residual. BWPM_GMRES=host runs the
+// Arnoldi steps from the host instead, waiting for each step's flag while the next one runs.
+template <typename T>
+void PlaneSolver<T>::gmres() {
   const long long m2 = 2 * static_cast<long long>(n());
   constexpr int m = kGmresRestart;
   const double tol = in_.gmres_tol;
@@ -875,19 +950,16 @@ void PlaneSolver<T>::gmres(int slot, int dir) {
     dot_partial_.alloc(kDotBlocks, stream_);
     flags_host_.alloc(m + 2);
     for (auto& e : gmres_events_) e.create();
+    gm_vblocks_ = static_cast<int>(ceil_div(m2, static_cast<long long>(kThreads)));
+    gm_dblocks_ = static_cast<int>(std::min<long long>(kDotBlocks, ceil_div(m2, 256LL)));
   }
+  const char* gm = std::getenv("BWPM_GMRES");
+  const bool host_loop = gm && std::strcmp(gm, "host") == 0;
+  if (!host_loop) build_cycle_graph();
   GmresState* st = gst_.ptr;
-  const int vblocks = static_cast<int>(ceil_div(m2, static_cast<long long>(kThreads)));
-  const int dblocks = static_cast<int>(std::min<long long>(kDotBlocks, ceil_div(m2, 256LL)));
-  auto dot_into = [&](const C* u, const C* v, cd* out) {
-    launch(k_dot_dev<T>, dim3(dblocks), dim3(256), 0, u, v, m2, dot_partial_.ptr, &st->counter, out);
-  };
-  auto apply = [&](const C* v, C* av) {  // av = v − G v/2
-    born_operator(v, av, slot, dir, 1);
-    ++gmres_applies_;
-  };
   auto host_norm = [&](const C* u) {  // ‖u‖ read back on the host
-    dot_into(u, u, &st->dot);
+    launch(k_dot_dev<T>, dim3(gm_dblocks_), dim3(256), 0, u, u, m2, dot_partial_.ptr, &st->counter,
+           &st->dot);
     cd d;
     check_cuda(cudaMemcpyAsync(&d, &st->dot, sizeof(cd), cudaMemcpyDeviceToHost, stream_), "dot");
     check_cuda(cudaStreamSynchronize(stream_), "dot");
@@ -897,49 +969,56 @@ void PlaneSolver<T>::gmres(int slot, int dir) {
   const double bnorm = host_norm(g_rhs_.ptr);
   if (bnorm == 0.0) return;
   for (int outer = 0; outer < 100; ++outer) {
-    apply(g_y_.ptr, g_w_.ptr);
+    born_operator(g_y_.ptr, g_w_.ptr, 1);
+    ++gmres_applies_;
     check_cuda(cudaMemcpyAsync(basis_[0].ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
     axpby(basis_[0].ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
     const double beta = host_norm(basis_[0].ptr);  // leaves the dot in st->dot
     if (beta <= tol * bnorm) return;
-    launch(k_norm_scale<T>, dim3(vblocks), dim3(kThreads), 0, basis_[0].ptr, (const C*)basis_[0].ptr,
-           (const cd*)&st->dot, &st->nrm, m2);
-    launch(k_gmres_start, dim3(1), dim3(64), 0, st);
+    launch(k_norm_scale<T>, dim3(gm_vblocks_), dim3(kThreads), 0, basis_[0].ptr,
+           (const C*)basis_[0].ptr, (const cd*)&st->dot, &st->nrm, m2);
+    launch(k_gmres_start, dim3(1), dim3(64), 0, st, tol * bnorm);
     int used = 0;
     bool done = false;
-    auto converged = [&](int j) {  // waits for the flag of Arnoldi step j
-      check_cuda(cudaEventSynchronize(gmres_events_[j]), "gmres flag");
-      return flags_host_.ptr[j] != 0;
-    };
-    for (int j = 0; j < m; ++j) {
-      apply(basis_[j].ptr, g_w_.ptr);
-      for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, h straight into the Hessenberg matrix
-        dot_into(basis_[i].ptr, g_w_.ptr, &st->h[i * m + j]);
-        launch(k_axpy_dev<T>, dim3(vblocks), dim3(kThreads), 0, g_w_.ptr, (const C*)basis_[i].ptr,
-               (const cd*)&st->h[i * m + j], -1.0, m2);
+    if (!host_loop) {
+      check_cuda(cudaGraphLaunch(cycle_.exec, stream_), "graph launch");
+      ++launches_;
+      check_cuda(cudaMemcpyAsync(flags_host_.ptr, st->flag, m * sizeof(int), cudaMemcpyDeviceToHost,
+                                 stream_), "flags");
+      check_cuda(cudaStreamSynchronize(stream_), "flags");
+      used = m;
+      for (int j = 0; j < m; ++j)
+        if (flags_host_.ptr[j]) {
+          used = j + 1;
+          done = true;
+          break;
+        }
+      gmres_applies_ += used;
+    } else {
+      auto converged = [&](int j) {  // waits for the flag of Arnoldi step j
+        check_cuda(cudaEventSynchronize(gmres_events_[j]), "gmres flag");
+        return flags_host_.ptr[j] != 0;
+      };
+      for (int j = 0; j < m; ++j) {
+        arnoldi_step(j, false, tol * bnorm);
+        ++gmres_applies_;
+        // step j is queued; the previous step's flag decides whether it counts
+        if (j > 0 && converged(j - 1)) {
+          used = j;
+          done = true;
+          break;
+        }
+        used = j + 1;
       }
-      dot_into(g_w_.ptr, g_w_.ptr, &st->dot);
-      launch(k_norm_scale<T>, dim3(vblocks), dim3(kThreads), 0, basis_[j + 1].ptr, (const C*)g_w_.ptr,
-             (const cd*)&st->dot, &st->nrm, m2);
-      launch(k_gmres_givens, dim3(1), dim3(32), 0, st, j, tol * bnorm);
-      check_cuda(cudaMemcpyAsync(flags_host_.ptr + j, &st->flag[j], sizeof(int), cudaMemcpyDeviceToHost,
-                                 stream_), "flag");
-      check_cuda(cudaEventRecord(gmres_events_[j], stream_), "event");
-      // step j is queued; the previous step's flag decides whether it counts
-      if (j > 0 && converged(j - 1)) {
-        used = j;
-        done = true;
-        break;
-      }
-      used = j + 1;
+      if (!done && converged(used - 1)) done = true;
     }
-    if (!done && converged(used - 1)) done = true;
     launch(k_gmres_backsolve, dim3(1), dim3(32), 0, st, used);
     for (int i = 0; i < used; ++i)
-      launch(k_axpy_dev<T>, dim3(vblocks), dim3(kThreads), 0, g_y_.ptr, (const C*)basis_[i].ptr,
+      launch(k_axpy_dev<T>, dim3(gm_vblocks_), dim3(kThreads), 0, g_y_.ptr, (const C*)basis_[i].ptr,
              (const cd*)&st->y[i], 1.0, m2);
     if (done) {
-      apply(g_y_.ptr, g_w_.ptr);
+      born_operator(g_y_.ptr, g_w_.ptr, 1);
+      ++gmres_applies_;
       check_cuda(cudaMemcpyAsync(g_tmp_.ptr, g_rhs_.ptr, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
       axpby(g_tmp_.ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
       if (host_norm(g_tmp_.ptr) <= tol * bnorm * 10.0) return;
@@ -954,9 +1033,11 @@ template <typename T>
 void PlaneSolver<T>::born_step(const C* spec, C* inc, int slot, int dir) {
   const BornGrid g = born_grid(slot);
   const long long nn = static_cast<long long>(n());
+  launch(k_set_born_cur<T>, dim3(1), dim3(32), 0, born_cur_.ptr,
+         BornCur<T>{g, dir, pot_.ptr + slot * nn});
   launch(k_born_half<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, spec, g_x_.ptr, g, 1.0);
-  born_operator(g_x_.ptr, g_rhs_.ptr, slot, dir);
-  gmres(slot, dir);
+  born_operator(g_x_.ptr, g_rhs_.ptr);
+  gmres();
   launch(k_born_half<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, (const C*)g_y_.ptr,
          g_y_.ptr, g, dir > 0 ? 1.0 : -1.0);
   fft_plane(g_y_.ptr, inc, 2, +1);

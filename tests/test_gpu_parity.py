@@ -239,3 +239,35 @@ def test_bulk_column_kernel_equals_plain_loads(core, monkeypatch, prefix, iters,
         assert np.array_equal(a[key], b[key]), key
     for q in (0, 5):
         assert np.array_equal(a["forward"][q], b["forward"][q])
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("prefix,iters", [("fluct1.", 1), ("fluct2.", 1), ("backscatter.", 3)])
+def test_gmres_cycle_graph_equals_host_loop(core, monkeypatch, prefix, iters, precision):
+    """The Born step's GMRES run as one CUDA graph per restart cycle (Arnoldi steps under
+    conditional nodes, the default) gives the same bits as the host-driven Arnoldi loop
+    (BWPM_GMRES=host): same kernels, same order, only who decides to stop differs."""
+    d = load_npz("random_volumes.npz")
+    args, field, fl = volume_case(d, prefix)
+    out = {}
+    for mode in ("host", "graph"):
+        monkeypatch.setenv("BWPM_GMRES", mode)
+        out[mode] = core.CudaSolver(*args, 0, fluctuation=fl, precision=precision).run(
+            field, iters, [])
+    for key in ("transmitted", "reflected"):
+        assert np.array_equal(out["host"][key], out["graph"][key]), key
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_gmres_cycle_graph_born2d(core, monkeypatch, precision):
+    """As above on a 2D Born chain (4096 points, 60 slabs with δn on every slab, 2 iterations)."""
+    from bwpm_b200 import workloads
+
+    p = workloads.born2d(nz=60, iterations=2)
+    out = {}
+    for mode in ("host", "graph"):
+        monkeypatch.setenv("BWPM_GMRES", mode)
+        out[mode] = core.CudaSolver(*p.core_args(), 0, fluctuation=p.fluctuation,
+                                    precision=precision).run(p.field, p.iterations, [])
+    for key in ("transmitted", "reflected"):
+        assert np.array_equal(out["host"][key], out["graph"][key]), key
