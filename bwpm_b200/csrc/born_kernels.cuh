@@ -40,15 +40,20 @@ __device__ __forceinline__ BornPoint born_point(const BornGrid& g, long long q) 
 
 // out = in · e^{i·sign·k_z·dz/2} on propagating waves, 0 elsewhere (P_½ and its inverse).
 template <typename T>
-__global__ void k_born_half(const cx<T>* in, cx<T>* out, BornGrid g, double sign) {
-  const long long n = static_cast<long long>(g.ny) * g.nx;
-  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (q >= n) return;
+__device__ __forceinline__ void born_half_at(long long q, const cx<T>* in, cx<T>* out,
+                                             const BornGrid& g, double sign) {
   const BornPoint p = born_point(g, q);
   cd f{0.0, 0.0};
   if (p.prop) f = cexp(cd{0.0, sign} * p.kz * (g.dz / 2.0));
   out[2 * q] = cast<T>(cast<double>(in[2 * q]) * f);
   out[2 * q + 1] = cast<T>(cast<double>(in[2 * q + 1]) * f);
+}
+
+template <typename T>
+__global__ void k_born_half(const cx<T>* in, cx<T>* out, BornGrid g, double sign) {
+  const long long n = static_cast<long long>(g.ny) * g.nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q < n) born_half_at(q, in, out, g, sign);
 }
 
 // The Born slab of the current step in device memory (grid with the slab's host index,
@@ -91,6 +96,15 @@ __global__ void k_born_prepare(const cx<T>* spec, cx<T>* w3, BornGrid g, int dir
   const long long n = static_cast<long long>(g.ny) * g.nx;
   const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (q < n) born_prepare_at(q, spec, w3, g, direction, distance);
+}
+
+// P_½ (signed = 0) or P_½^{±} with the sign of the current slab's direction (signed = 1).
+template <typename T>
+__global__ void k_born_half_cur(const cx<T>* in, cx<T>* out, const BornCur<T>* cur, int signed_) {
+  const BornGrid g = cur->g;
+  const long long n = static_cast<long long>(g.ny) * g.nx;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q < n) born_half_at(q, in, out, g, signed_ && cur->dir <= 0 ? -1.0 : 1.0);
 }
 
 template <typename T>

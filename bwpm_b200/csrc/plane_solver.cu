@@ -9,6 +9,7 @@
 // - selection, mask, reflection gather and sparse source add are fused into the inverse
 //   transform's epilogue; interface pixel lists and source stores are allocated once.
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -83,7 +84,8 @@ class PlaneSolver final : public Solver {
   void born_emission(int slot, int dir, C* plane);
   void gmres();
   void arnoldi_step(int j, bool in_graph, double tol_bnorm);
-  void build_cycle_graph();
+  void gmres_alloc();
+  void build_born_graph();
   // the forward/backward sweeps of a run (device work only, unless Born slabs need GMRES)
   void sweeps(int iterations, const std::vector<int>& keep_slot, DevBuf<C>& kept_f, DevBuf<C>& kept_b,
               DevBuf<C>& t_iter, DevBuf<C>& r_iter);
@@ -130,8 +132,10 @@ class PlaneSolver final : public Solver {
   std::vector<DevBuf<C>> basis_;
   DevBuf<GmresState> gst_;
   DevBuf<BornCur<T>> born_cur_;  // the Born slab of the current step (set per step)
-  OwnedGraph cycle_;             // one GMRES restart cycle (Arnoldi steps under conditionals)
-  cudaGraphConditionalHandle cycle_cond_[kGmresRestart] = {};  // one per step's node
+  OwnedGraph born_graph_;        // one Born step: P_½, right-hand side, GMRES, P_½^{±}, F⁻¹
+  GmresConds conds_{};           // its conditional nodes' handles
+  DevBuf<C*> basis_ptrs_;        // the Krylov basis vectors' addresses (device)
+  bool born_graph_used_ = false; // a run launched it: its error flag and counts are read at the end
   int gm_vblocks_ = 0, gm_dblocks_ = 0;
   DevBuf<cd> dot_partial_;
   PinnedBuf<int> flags_host_;
@@ -513,7 +517,7 @@ void PlaneSolver<T>::setup() {
         upload_rf(rf_x_, static_cast<int>(in_.nx), tw_rf_x_);
         check_cuda(cudaFuncSetAttribute((const void*)rf_y_.cols,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(rf_y_.smem)), "smem");
+                                        static_cast<int>(rf_y_.cols_smem)), "smem");
         check_cuda(cudaFuncSetAttribute((const void*)rf_x_.rows,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(rf_x_.smem)), "smem");
@@ -752,7 +756,7 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
     if (rf_y_.cols) {
       ColStep<float> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, 0,
                        status_.ptr};
-      launch(rf_y_.cols, dim3(nx / rf_y_.lines), dim3(kRfThreads), rf_y_.smem, c, ps, npass,
+      launch(rf_y_.cols, dim3(nx / rf_y_.lines), dim3(kRfThreads), rf_y_.cols_smem, c, ps, npass,
              (const Tw<float>*)tw_rf_y_.ptr);
       RowSelect<float> r;
       r.work = work_.ptr;
@@ -887,9 +891,7 @@ void PlaneSolver<T>::arnoldi_step(int j, bool in_graph, double tol_bnorm) {
   launch(k_norm_scale<T>, dim3(gm_vblocks_), dim3(kThreads), 0, basis_[j + 1].ptr,
          (const C*)g_w_.ptr, (const cd*)&st->dot, &st->nrm, m2);
   if (in_graph) {
-    const bool has_next = j + 1 < kGmresRestart;
-    launch(k_gmres_givens_cond, dim3(1), dim3(32), 0, st, j,
-           has_next ? cycle_cond_[j + 1] : cudaGraphConditionalHandle{0}, has_next ? 1 : 0);
+    launch(k_gmres_givens_cond, dim3(1), dim3(32), 0, st, j, conds_);
   } else {
     launch(k_gmres_givens, dim3(1), dim3(32), 0, st, j, tol_bnorm);
     check_cuda(cudaMemcpyAsync(flags_host_.ptr + j, &st->flag[j], sizeof(int), cudaMemcpyDeviceToHost,
@@ -898,64 +900,156 @@ void PlaneSolver<T>::arnoldi_step(int j, bool in_graph, double tol_bnorm) {
   }
 }
 
-// The restart cycle as one graph, built once per solver (the buffers it names are fixed; the
-// slab comes from born_cur_, the tolerance from the state): Arnoldi step j runs under an IF node
-// with a handle of its own (a handle serves one node). Step 0's condition is 1 at each launch,
-// the others 0 until step j − 1 sets them, which it does unless it converged; a skipped step sets
-// nothing, so every later step is skipped too.
 template <typename T>
-void PlaneSolver<T>::build_cycle_graph() {
-  if (cycle_.exec) return;
+void PlaneSolver<T>::gmres_alloc() {
+  if (!basis_.empty()) return;
+  const long long m2 = 2 * static_cast<long long>(n());
+  constexpr int m = kGmresRestart;
+  for (int i = 0; i <= m; ++i) basis_.emplace_back(static_cast<std::size_t>(m2), stream_);
+  std::vector<C*> ptrs;
+  for (auto& b : basis_) ptrs.push_back(b.ptr);
+  basis_ptrs_.alloc(ptrs.size(), stream_);
+  basis_ptrs_.upload(ptrs.data(), ptrs.size());
+  gst_.alloc(1, stream_);
+  check_cuda(cudaMemsetAsync(gst_.ptr, 0, sizeof(GmresState), stream_), "memset");
+  dot_partial_.alloc(kDotBlocks, stream_);
+  flags_host_.alloc(m + 2);
+  for (auto& e : gmres_events_) e.create();
+  gm_vblocks_ = static_cast<int>(ceil_div(m2, static_cast<long long>(kThreads)));
+  gm_dblocks_ = static_cast<int>(std::min<long long>(kDotBlocks, ceil_div(m2, 256LL)));
+}
+
+// The Born step of born_step (P_½, right-hand side, GMRES(30), P_½^{±}, inverse transform) as
+// one CUDA graph, built once per solver: the buffers it names are fixed, the slab comes from
+// born_cur_ and the tolerance from the state, so one graph serves every Born slab and both
+// directions. The host loop's decisions become conditional nodes (a handle per node) set by
+// one-thread kernels (gmres_kernels.cuh) with the same FP64 comparisons:
+//   P_½, G·x, y = rhs, ‖rhs‖ → init
+//   WHILE active:  A·y, β → restart
+//     IF cycle:    v_0 = r/β, g; arm; IF step_0 {Arnoldi 0} … IF step_29 {Arnoldi 29};
+//                  cycle_done; back substitution; y += Σ y_i v_i
+//       IF done:   A·y, ‖rhs − A·y‖ → final
+//   P_½^{±}, F⁻¹
+// The host launches it after writing the slab record and waits for nothing.
+template <typename T>
+void PlaneSolver<T>::build_born_graph() {
+  if (born_graph_.exec) return;
   const std::int64_t launches = launches_;
-  check_cuda(cudaGraphCreate(&cycle_.g, 0), "graph create");
-  for (int j = 0; j < kGmresRestart; ++j)
-    check_cuda(cudaGraphConditionalHandleCreate(&cycle_cond_[j], cycle_.g, j == 0 ? 1u : 0u,
-                                                cudaGraphCondAssignDefault),
+  const long long nn = static_cast<long long>(n());
+  const long long m2 = 2 * nn;
+  GmresState* st = gst_.ptr;
+  cudaGraph_t top = nullptr;
+  check_cuda(cudaGraphCreate(&top, 0), "graph create");
+  born_graph_.g = top;
+  auto handle = [&](cudaGraphConditionalHandle& h) {
+    check_cuda(cudaGraphConditionalHandleCreate(&h, top, 0u, cudaGraphCondAssignDefault),
                "conditional handle");
-  cudaGraphNode_t prev = nullptr;
-  for (int j = 0; j < kGmresRestart; ++j) {
+  };
+  handle(conds_.active);
+  handle(conds_.cycle);
+  handle(conds_.done);
+  for (auto& h : conds_.step) handle(h);
+  // captures what `f` enqueues into graph g after `deps`; returns the capture's last nodes
+  auto capture = [&](cudaGraph_t g, std::vector<cudaGraphNode_t> deps, auto&& f) {
+    check_cuda(cudaStreamBeginCaptureToGraph(stream_, g, deps.empty() ? nullptr : deps.data(),
+                                             nullptr, deps.size(),
+                                             cudaStreamCaptureModeThreadLocal),
+               "capture");
+    f();
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* last = nullptr;
+    std::size_t nlast = 0;
+    check_cuda(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, nullptr, &last, &nlast), "capture");
+    std::vector<cudaGraphNode_t> out(last, last + nlast);
+    cudaGraph_t g2;
+    check_cuda(cudaStreamEndCapture(stream_, &g2), "capture");
+    return out;
+  };
+  // adds a conditional node after `deps`; returns it and its body
+  auto conditional = [&](cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+                         cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                         cudaGraph_t& body) {
     cudaGraphNodeParams p = {};
     p.type = cudaGraphNodeTypeConditional;
-    p.conditional.handle = cycle_cond_[j];
-    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.handle = h;
+    p.conditional.type = type;
     p.conditional.size = 1;
     cudaGraphNode_t node;
-    check_cuda(cudaGraphAddNode(&node, cycle_.g, prev ? &prev : nullptr, prev ? 1 : 0, &p),
+    check_cuda(cudaGraphAddNode(&node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &p),
                "conditional node");
-    check_cuda(cudaStreamBeginCaptureToGraph(stream_, p.conditional.phGraph_out[0], nullptr,
-                                             nullptr, 0, cudaStreamCaptureModeThreadLocal),
-               "capture");
-    arnoldi_step(j, true, 0.0);
-    cudaGraph_t body;
-    check_cuda(cudaStreamEndCapture(stream_, &body), "capture");
-    prev = node;
+    body = p.conditional.phGraph_out[0];
+    return std::vector<cudaGraphNode_t>{node};
+  };
+  const BornCur<T>* cur = born_cur_.ptr;
+  const dim3 pts(ceil_div(nn, kThreads)), vec(gm_vblocks_), blk(kThreads);
+  auto dot = [&](const C* u, const C* v, cd* out) {
+    launch(k_dot_dev<T>, dim3(gm_dblocks_), dim3(256), 0, u, v, m2, dot_partial_.ptr, &st->counter,
+           out);
+  };
+  auto copy = [&](C* dst, const C* src) {
+    check_cuda(cudaMemcpyAsync(dst, src, m2 * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
+  };
+  std::vector<cudaGraphNode_t> d = capture(top, {}, [&] {
+    launch(k_born_half_cur<T>, pts, blk, 0, (const C*)spec_.ptr, g_x_.ptr, cur, 0);
+    born_operator(g_x_.ptr, g_rhs_.ptr);
+    copy(g_y_.ptr, g_rhs_.ptr);
+    dot(g_rhs_.ptr, g_rhs_.ptr, &st->dot);
+    launch(k_gmres_init, dim3(1), dim3(32), 0, st, in_.gmres_tol, conds_);
+  });
+  cudaGraph_t wbody, cbody, dbody;
+  d = conditional(top, d, conds_.active, cudaGraphCondTypeWhile, wbody);
+  std::vector<cudaGraphNode_t> w = capture(wbody, {}, [&] {
+    born_operator(g_y_.ptr, g_w_.ptr, 1);
+    copy(basis_[0].ptr, g_rhs_.ptr);
+    axpby(basis_[0].ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
+    dot(basis_[0].ptr, basis_[0].ptr, &st->dot);
+    launch(k_gmres_restart, dim3(1), dim3(32), 0, st, conds_);
+  });
+  conditional(wbody, w, conds_.cycle, cudaGraphCondTypeIf, cbody);
+  std::vector<cudaGraphNode_t> c = capture(cbody, {}, [&] {
+    launch(k_norm_scale<T>, vec, blk, 0, basis_[0].ptr, (const C*)basis_[0].ptr,
+           (const cd*)&st->dot, &st->nrm, m2);
+    launch(k_gmres_start, dim3(1), dim3(64), 0, st, -1.0);
+    launch(k_gmres_arm, dim3(1), dim3(32), 0, conds_);
+  });
+  for (int j = 0; j < kGmresRestart; ++j) {
+    cudaGraph_t sbody;
+    c = conditional(cbody, c, conds_.step[j], cudaGraphCondTypeIf, sbody);
+    capture(sbody, {}, [&] { arnoldi_step(j, true, 0.0); });
   }
-  check_cuda(cudaGraphInstantiate(&cycle_.exec, cycle_.g, 0), "instantiate");
+  c = capture(cbody, c, [&] {
+    launch(k_gmres_cycle_done, dim3(1), dim3(32), 0, st, conds_);
+    launch(k_gmres_backsolve, dim3(1), dim3(32), 0, st, -1);
+    launch(k_axpy_basis<T>, vec, blk, 0, g_y_.ptr, (C* const*)basis_ptrs_.ptr, (const GmresState*)st,
+           m2);
+  });
+  conditional(cbody, c, conds_.done, cudaGraphCondTypeIf, dbody);
+  capture(dbody, {}, [&] {
+    born_operator(g_y_.ptr, g_w_.ptr, 1);
+    copy(g_tmp_.ptr, g_rhs_.ptr);
+    axpby(g_tmp_.ptr, g_w_.ptr, cd{-1.0, 0.0}, cd{1.0, 0.0}, m2);
+    dot(g_tmp_.ptr, g_tmp_.ptr, &st->dot);
+    launch(k_gmres_final, dim3(1), dim3(32), 0, st, conds_);
+  });
+  capture(top, d, [&] {
+    launch(k_born_half_cur<T>, pts, blk, 0, (const C*)g_y_.ptr, g_y_.ptr, cur, 1);
+    fft_plane(g_y_.ptr, inc_.ptr, 2, +1);
+  });
+  check_cuda(cudaGraphInstantiate(&born_graph_.exec, top, 0), "instantiate");
   launches_ = launches;
 }
 
 // GMRES(30) for (1 − G/2)·y = rhs with start y = rhs (cpp/src/solver.cpp:130-207, :336-342),
-// scalar work on the device (gmres_kernels.cuh). The host waits on the device for ‖rhs‖ once per
-// solve and per restart for β, the cycle's flags and the final residual. BWPM_GMRES=host runs the
-// Arnoldi steps from the host instead, waiting for each step's flag while the next one runs.
+// driven from the host (BWPM_GMRES=host; the default runs the whole Born step as the graph of
+// build_born_graph): scalar work on the device (gmres_kernels.cuh), the host waiting for ‖rhs‖,
+// per restart for β and the final residual, and per Arnoldi step for the previous step's flag
+// while the next one runs.
 template <typename T>
 void PlaneSolver<T>::gmres() {
   const long long m2 = 2 * static_cast<long long>(n());
   constexpr int m = kGmresRestart;
   const double tol = in_.gmres_tol;
-  if (basis_.empty()) {
-    for (int i = 0; i <= m; ++i) basis_.emplace_back(static_cast<std::size_t>(m2), stream_);
-    gst_.alloc(1, stream_);
-    check_cuda(cudaMemsetAsync(gst_.ptr, 0, sizeof(GmresState), stream_), "memset");
-    dot_partial_.alloc(kDotBlocks, stream_);
-    flags_host_.alloc(m + 2);
-    for (auto& e : gmres_events_) e.create();
-    gm_vblocks_ = static_cast<int>(ceil_div(m2, static_cast<long long>(kThreads)));
-    gm_dblocks_ = static_cast<int>(std::min<long long>(kDotBlocks, ceil_div(m2, 256LL)));
-  }
-  const char* gm = std::getenv("BWPM_GMRES");
-  const bool host_loop = gm && std::strcmp(gm, "host") == 0;
-  if (!host_loop) build_cycle_graph();
+  gmres_alloc();
   GmresState* st = gst_.ptr;
   auto host_norm = [&](const C* u) {  // ‖u‖ read back on the host
     launch(k_dot_dev<T>, dim3(gm_dblocks_), dim3(256), 0, u, u, m2, dot_partial_.ptr, &st->counter,
@@ -980,38 +1074,22 @@ void PlaneSolver<T>::gmres() {
     launch(k_gmres_start, dim3(1), dim3(64), 0, st, tol * bnorm);
     int used = 0;
     bool done = false;
-    if (!host_loop) {
-      check_cuda(cudaGraphLaunch(cycle_.exec, stream_), "graph launch");
-      ++launches_;
-      check_cuda(cudaMemcpyAsync(flags_host_.ptr, st->flag, m * sizeof(int), cudaMemcpyDeviceToHost,
-                                 stream_), "flags");
-      check_cuda(cudaStreamSynchronize(stream_), "flags");
-      used = m;
-      for (int j = 0; j < m; ++j)
-        if (flags_host_.ptr[j]) {
-          used = j + 1;
-          done = true;
-          break;
-        }
-      gmres_applies_ += used;
-    } else {
-      auto converged = [&](int j) {  // waits for the flag of Arnoldi step j
-        check_cuda(cudaEventSynchronize(gmres_events_[j]), "gmres flag");
-        return flags_host_.ptr[j] != 0;
-      };
-      for (int j = 0; j < m; ++j) {
-        arnoldi_step(j, false, tol * bnorm);
-        ++gmres_applies_;
-        // step j is queued; the previous step's flag decides whether it counts
-        if (j > 0 && converged(j - 1)) {
-          used = j;
-          done = true;
-          break;
-        }
-        used = j + 1;
+    auto converged = [&](int j) {  // waits for the flag of Arnoldi step j
+      check_cuda(cudaEventSynchronize(gmres_events_[j]), "gmres flag");
+      return flags_host_.ptr[j] != 0;
+    };
+    for (int j = 0; j < m; ++j) {
+      arnoldi_step(j, false, tol * bnorm);
+      ++gmres_applies_;
+      // step j is queued; the previous step's flag decides whether it counts
+      if (j > 0 && converged(j - 1)) {
+        used = j;
+        done = true;
+        break;
       }
-      if (!done && converged(used - 1)) done = true;
+      used = j + 1;
     }
+    if (!done && converged(used - 1)) done = true;
     launch(k_gmres_backsolve, dim3(1), dim3(32), 0, st, used);
     for (int i = 0; i < used; ++i)
       launch(k_axpy_dev<T>, dim3(gm_vblocks_), dim3(kThreads), 0, g_y_.ptr, (const C*)basis_[i].ptr,
@@ -1035,6 +1113,15 @@ void PlaneSolver<T>::born_step(const C* spec, C* inc, int slot, int dir) {
   const long long nn = static_cast<long long>(n());
   launch(k_set_born_cur<T>, dim3(1), dim3(32), 0, born_cur_.ptr,
          BornCur<T>{g, dir, pot_.ptr + slot * nn});
+  const char* gm = std::getenv("BWPM_GMRES");
+  if (!(gm && std::strcmp(gm, "host") == 0) && spec == spec_.ptr && inc == inc_.ptr) {
+    gmres_alloc();
+    build_born_graph();
+    check_cuda(cudaGraphLaunch(born_graph_.exec, stream_), "graph launch");
+    ++launches_;
+    born_graph_used_ = true;
+    return;
+  }
   launch(k_born_half<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, spec, g_x_.ptr, g, 1.0);
   born_operator(g_x_.ptr, g_rhs_.ptr);
   gmres();
@@ -1188,6 +1275,16 @@ void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* ke
   }
   out.stored_values = iterations > 0 ? 2 * iface_total_ : 0;
   check_cuda(cudaStreamSynchronize(stream_), "synchronize");
+  if (born_graph_used_) {
+    born_graph_used_ = false;
+    GmresState hs;
+    check_cuda(cudaMemcpy(&hs, gst_.ptr, sizeof(GmresState), cudaMemcpyDeviceToHost), "gmres state");
+    gmres_applies_ += hs.applies;
+    char* base = reinterpret_cast<char*>(gst_.ptr);
+    check_cuda(cudaMemset(base + offsetof(GmresState, err), 0, sizeof(int)), "gmres state");
+    check_cuda(cudaMemset(base + offsetof(GmresState, applies), 0, sizeof(long long)), "gmres state");
+    if (hs.err) throw std::runtime_error("GMRES did not converge in the Born step (CUDA)");
+  }
   if (status_.ptr) {
     int st = 0;
     check_cuda(cudaMemcpy(&st, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost), "status");

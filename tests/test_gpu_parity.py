@@ -243,9 +243,9 @@ def test_bulk_column_kernel_equals_plain_loads(core, monkeypatch, prefix, iters,
 
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("prefix,iters", [("fluct1.", 1), ("fluct2.", 1), ("backscatter.", 3)])
-def test_gmres_cycle_graph_equals_host_loop(core, monkeypatch, prefix, iters, precision):
-    """The Born step's GMRES run as one CUDA graph per restart cycle (Arnoldi steps under
-    conditional nodes, the default) gives the same bits as the host-driven Arnoldi loop
+def test_born_step_graph_equals_host_loop(core, monkeypatch, prefix, iters, precision):
+    """The Born step run as one CUDA graph whose conditional nodes make the GMRES decisions on
+    the device (the default) gives the same bits as the host-driven GMRES loop
     (BWPM_GMRES=host): same kernels, same order, only who decides to stop differs."""
     d = load_npz("random_volumes.npz")
     args, field, fl = volume_case(d, prefix)
@@ -259,7 +259,7 @@ def test_gmres_cycle_graph_equals_host_loop(core, monkeypatch, prefix, iters, pr
 
 
 @pytest.mark.parametrize("precision", [64, 32])
-def test_gmres_cycle_graph_born2d(core, monkeypatch, precision):
+def test_born_step_graph_born2d(core, monkeypatch, precision):
     """As above on a 2D Born chain (4096 points, 60 slabs with δn on every slab, 2 iterations)."""
     from bwpm_b200 import workloads
 
