@@ -38,6 +38,12 @@ __device__ __forceinline__ BornPoint born_point(const BornGrid& g, long long q) 
   return p;
 }
 
+// a·x + b·y in FP64, stored in T (the vector update of k_axpby).
+template <typename T>
+__device__ __forceinline__ cx<T> axpby_at(cd a, cx<T> x, cd b, cx<T> y) {
+  return cast<T>(a * cast<double>(x) + b * cast<double>(y));
+}
+
 // out = in · e^{i·sign·k_z·dz/2} on propagating waves, 0 elsewhere (P_½ and its inverse).
 template <typename T>
 __device__ __forceinline__ void born_half_at(long long q, const cx<T>* in, cx<T>* out,
@@ -158,12 +164,19 @@ __global__ void k_born_finish(const cx<T>* w3, cx<T>* out, BornGrid g, int direc
   if (q < n) born_finish_at(q, w3, out, g, direction);
 }
 
+// With `in` (the operator of the Cayley step, A = 1 − G/2): out = in − G·in/2, in the
+// arithmetic of k_axpby(out ← in, G·in, −½, 1) on G·in stored in T.
 template <typename T>
-__global__ void k_born_finish_cur(const cx<T>* w3, cx<T>* out, const BornCur<T>* cur) {
+__global__ void k_born_finish_cur(const cx<T>* w3, cx<T>* out, const BornCur<T>* cur,
+                                  const cx<T>* in) {
   const BornGrid g = cur->g;
   const long long n = static_cast<long long>(g.ny) * g.nx;
   const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (q < n) born_finish_at(q, w3, out, g, cur->dir);
+  if (q >= n) return;
+  born_finish_at(q, w3, out, g, cur->dir);
+  if (in)
+    for (int c = 0; c < 2; ++c)
+      out[2 * q + c] = axpby_at(cd{-0.5, 0.0}, out[2 * q + c], cd{1.0, 0.0}, in[2 * q + c]);
 }
 
 // total = Σ_m ½·e^{i d′k_z(1−ζ_m)dz}·i dz/(2k_z)·[P(k_d′)·Ŝ_m]⊥ (spectrum), sources (2, N, 3).
@@ -203,7 +216,7 @@ __global__ void k_axpby(cx<T>* y, const cx<T>* x, cd a, cd b, long long m) {
   // y = a·x + b·y
   const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (i >= m) return;
-  y[i] = cast<T>(a * cast<double>(x[i]) + b * cast<double>(y[i]));
+  y[i] = axpby_at(a, x[i], b, y[i]);
 }
 
 // ---- transforms of planes with ncomp interleaved components ---------------------------------

@@ -66,18 +66,6 @@ constexpr std::size_t rf_smem() {
   return static_cast<std::size_t>(rf_lines<N>()) * 4 * rf::padded(N) * sizeof(cf);
 }
 
-// The column kernel keeps a line's spectrum (both components) in shared memory beside its
-// exchange buffers where two CTAs per SM still fit; else in registers (lengths 3·2^k).
-template <int N>
-constexpr bool rf_spec_smem() {
-  return rf_lines<N>() * (4 * rf::padded(N) + 2 * N) * sizeof(cf) <= 113 * 1024;
-}
-template <int N>
-constexpr std::size_t rf_cols_smem() {
-  return rf_smem<N>() +
-         (rf_spec_smem<N>() ? static_cast<std::size_t>(rf_lines<N>()) * 2 * N * sizeof(cf) : 0);
-}
-
 namespace rfp {
 
 // One stage on both components (a, b) of a line: rf::stage with the twiddle shared.
@@ -185,18 +173,17 @@ __global__ void __launch_bounds__(kRfThreads, 2)
       a.spec_out[2 * q] = sx[m];
       a.spec_out[2 * q + 1] = sy[m];
     }
-  // pass j: operator product of (ax, ay) into (ox, oy) (which may be the same arrays), inverse
-  // y transform, store into the pass's work plane
-  auto pass = [&](int j, cf (&ax)[E], cf (&ay)[E], cf (&ox)[E], cf (&oy)[E]) {
+  for (int j = 0; j < npass; ++j) {
     const PassRec pr = ps[j];
     const cf* tab = static_cast<const cf*>(pr.tab);
+    cf wx[E], wy[E];
     if (pr.scalar) {
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const long long q = static_cast<long long>(x) * NY + t + m * NT;
         const cf hi = tab[q], lo = tab[n + q];
-        ox[m] = pmul(ax[m], hi, lo);
-        oy[m] = pmul(ay[m], hi, lo);
+        wx[m] = pmul(sx[m], hi, lo);
+        wy[m] = pmul(sy[m], hi, lo);
       }
     } else {
 #pragma unroll
@@ -205,48 +192,17 @@ __global__ void __launch_bounds__(kRfThreads, 2)
         cf tv[6];
 #pragma unroll
         for (int b = 0; b < 6; ++b) tv[b] = tab[b * n + q];
-        const cf a0 = ax[m], a1 = ay[m];
-        ox[m] = tmul_v(a0, tv, 0) + tmul_v(a1, tv, 1);
-        oy[m] = tmul_v(a0, tv, 1) + tmul_v(a1, tv, 2);
+        wx[m] = tmul_v(sx[m], tv, 0) + tmul_v(sy[m], tv, 1);
+        wy[m] = tmul_v(sx[m], tv, 1) + tmul_v(sy[m], tv, 2);
         // the table values of four points in flight at a time
         if (m % 4 == 3) asm volatile("" ::: "memory");
       }
     }
-    rfp::fft2<+1, NY>(ox, oy, buf, phase, tw, t, typename PlaneRf<NY>::R{});
+    rfp::fft2<+1, NY>(wx, wy, buf, phase, tw, t, typename PlaneRf<NY>::R{});
     cf* w = a.work + static_cast<long long>(j) * 2 * n;
 #pragma unroll
     for (int m = 0; m < E; ++m)
-      st_px(w + (static_cast<long long>(x) * NY + t + m * NT) * 2, ox[m], oy[m]);
-  };
-  if constexpr (rf_spec_smem<NY>()) {
-    // several passes: the spectrum waits in shared memory (each thread its own points, no
-    // barrier) and each pass transforms a fresh copy in place, so no transform holds it in
-    // registers; one pass: in place in the registers
-    if (npass > 1) {
-      cf* spec = sm + static_cast<long long>(rf_lines<NY>()) * 4 * P +
-                 static_cast<long long>(line) * 2 * NY;
-#pragma unroll
-      for (int m = 0; m < E; ++m) {
-        spec[t + m * NT] = sx[m];
-        spec[NY + t + m * NT] = sy[m];
-      }
-      for (int j = 0; j < npass; ++j) {
-        cf ax[E], ay[E];
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-          ax[m] = spec[t + m * NT];
-          ay[m] = spec[NY + t + m * NT];
-        }
-        pass(j, ax, ay, ax, ay);
-      }
-    } else if (npass == 1) {
-      pass(0, sx, sy, sx, sy);
-    }
-  } else {
-    for (int j = 0; j < npass; ++j) {
-      cf wx[E], wy[E];
-      pass(j, sx, sy, wx, wy);
-    }
+      st_px(w + (static_cast<long long>(x) * NY + t + m * NT) * 2, wx[m], wy[m]);
   }
 }
 
@@ -365,9 +321,8 @@ using RowsRfFn = void (*)(RowSelect<float>, const PassRec*, int, const Tw<float>
 struct RfKernels {
   ColsRfFn cols = nullptr;
   RowsRfFn rows = nullptr;
-  int lines = 0;               // lines per CTA
-  std::size_t cols_smem = 0;   // shared memory per CTA of the column kernel
-  std::size_t smem = 0;        // of the row kernel
+  int lines = 0;          // lines per CTA
+  std::size_t smem = 0;   // shared memory per CTA
   std::vector<int> radices;
 };
 
@@ -378,7 +333,7 @@ inline std::vector<int> radix_list(rf::Radices<Rs...>) {
 
 template <int N>
 inline RfKernels rf_kernels_of() {
-  return {k_cols_rf<N>, k_rows_rf<N>, rf_lines<N>(), rf_cols_smem<N>(), rf_smem<N>(),
+  return {k_cols_rf<N>, k_rows_rf<N>, rf_lines<N>(), rf_smem<N>(),
           radix_list(typename PlaneRf<N>::R{})};
 }
 

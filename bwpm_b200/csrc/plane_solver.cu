@@ -128,7 +128,7 @@ class PlaneSolver final : public Solver {
   // Born
   std::vector<cd> hosts_;
   DevBuf<C> pot_, born_fwd_, born_bwd_, w3_, t3_, sources_, g_x_, g_rhs_, g_y_, g_w_, g_tmp_,
-      g_tmp2_, inc_;
+      inc_;
   std::vector<DevBuf<C>> basis_;
   DevBuf<GmresState> gst_;
   DevBuf<BornCur<T>> born_cur_;  // the Born slab of the current step (set per step)
@@ -517,7 +517,7 @@ void PlaneSolver<T>::setup() {
         upload_rf(rf_x_, static_cast<int>(in_.nx), tw_rf_x_);
         check_cuda(cudaFuncSetAttribute((const void*)rf_y_.cols,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(rf_y_.cols_smem)), "smem");
+                                        static_cast<int>(rf_y_.smem)), "smem");
         check_cuda(cudaFuncSetAttribute((const void*)rf_x_.rows,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(rf_x_.smem)), "smem");
@@ -548,7 +548,7 @@ void PlaneSolver<T>::setup() {
     w3_.alloc(3 * nn, stream_);
     t3_.alloc(3 * nn, stream_);
     sources_.alloc(6 * nn, stream_);
-    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &g_tmp2_, &inc_}) b->alloc(2 * nn, stream_);
+    for (auto* b : {&g_x_, &g_rhs_, &g_y_, &g_w_, &g_tmp_, &inc_}) b->alloc(2 * nn, stream_);
   }
   check_cuda(cudaStreamSynchronize(stream_), "setup");  // this solver's stream only
 }
@@ -756,7 +756,7 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
     if (rf_y_.cols) {
       ColStep<float> c{xbuf_.ptr, work_.ptr, want_spec ? spec_.ptr : nullptr, ny, nx, 0,
                        status_.ptr};
-      launch(rf_y_.cols, dim3(nx / rf_y_.lines), dim3(kRfThreads), rf_y_.cols_smem, c, ps, npass,
+      launch(rf_y_.cols, dim3(nx / rf_y_.lines), dim3(kRfThreads), rf_y_.smem, c, ps, npass,
              (const Tw<float>*)tw_rf_y_.ptr);
       RowSelect<float> r;
       r.work = work_.ptr;
@@ -848,13 +848,9 @@ void PlaneSolver<T>::born_operator(const C* in, C* out, int combine) {
   launch(k_born_potential_cur<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0, w3_.ptr, cur,
          nn, static_cast<T>(1.0 / static_cast<double>(nn)));
   fft_plane(w3_.ptr, w3_.ptr, 3, -1);
+  // combine: out = in − G·in/2 in the same kernel
   launch(k_born_finish_cur<T>, dim3(ceil_div(nn, kThreads)), dim3(kThreads), 0,
-         (const C*)w3_.ptr, out, cur);
-  if (combine) {  // out = in − G·in/2
-    check_cuda(cudaMemcpyAsync(g_tmp2_.ptr, out, 2 * nn * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
-    check_cuda(cudaMemcpyAsync(out, in, 2 * nn * sizeof(C), cudaMemcpyDeviceToDevice, stream_), "copy");
-    axpby(out, g_tmp2_.ptr, cd{-0.5, 0.0}, cd{1.0, 0.0}, 2 * nn);
-  }
+         (const C*)w3_.ptr, out, cur, combine ? in : (const C*)nullptr);
 }
 
 template <typename T>
