@@ -221,23 +221,28 @@ __global__ void k_axpby(cx<T>* y, const cx<T>* x, cd a, cd b, long long m) {
 
 // ---- transforms of planes with ncomp interleaved components ---------------------------------
 
-// nx = 1: one CTA per component, the whole line in shared memory.
-template <int DIR, typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_line_fft(const cx<T>* in, cx<T>* out, int n, int ncomp, FftPlan plan,
-                           const Tw<T>* __restrict__ tw) {
+// nx = 1: one CTA per component, the whole line in shared memory. A launch has ncomp CTAs, so
+// a transform's latency is the cost: the stages are expanded in the kernel (no register saves
+// through local memory per stage), 128 registers, and EPT values per thread (8 where the
+// threads allow it: twice the warps of 16).
+template <int DIR, typename T, int EPT = 16>
+__global__ void __launch_bounds__(kPlaneThreads, 1)
+    k_line_fft(const cx<T>* in, cx<T>* out, int n, int ncomp, const __grid_constant__ FftPlan plan,
+               const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   for (int q = tid; q < n; q += nt) buf[q] = in[static_cast<long long>(q) * ncomp + c];
   __syncthreads();
-  fft_smem<DIR>(buf, plan, tw, 1, tid, nt);
+  fft_smem_inline<DIR, EPT>(buf, plan, tw, 1, tid, nt);
   for (int q = tid; q < n; q += nt) out[static_cast<long long>(q) * ncomp + c] = buf[q];
 }
 
 // y transform of `cols` columns × ncomp components per CTA; smem [y][col][comp].
 template <int DIR, typename T>
-__global__ void __launch_bounds__(kPlaneThreads) k_cols_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int cols,
-                           FftPlan plan, const Tw<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks<T>)
+    k_cols_fft(const cx<T>* in, cx<T>* out, int ny, int nx, int ncomp, int cols,
+               const __grid_constant__ FftPlan plan, const Tw<T>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
   const int x0 = blockIdx.x * cols;
@@ -249,7 +254,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_cols_fft(const cx<T>* in, cx<
     buf[idx] = x < nx ? in[(static_cast<long long>(y) * nx + x) * ncomp + c] : cx<T>{0, 0};
   }
   __syncthreads();
-  fft_smem<DIR>(buf, plan, tw, lane, tid, nt);
+  fft_smem_inline<DIR>(buf, plan, tw, lane, tid, nt);
   for (int idx = tid; idx < tile; idx += nt) {
     const int y = idx / lane, rem = idx - y * lane;
     const int x = x0 + rem / ncomp, c = rem % ncomp;

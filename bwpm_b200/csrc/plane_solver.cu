@@ -142,6 +142,7 @@ class PlaneSolver final : public Solver {
   OwnedEvent gmres_events_[kGmresRestart];
   // launch shapes
   int thr2d_ = 32, thr_line3_ = 32;
+  bool line_ept8_ = false;  // 2D line transforms with 8 values per thread (k_line_fft)
   int sms_ = 148;
   LaunchShape rows2_, rows3_, sel_, cols1_, cols2_, cols3_;
   std::int64_t launches_ = 0, gmres_applies_ = 0;
@@ -334,8 +335,11 @@ void PlaneSolver<T>::setup() {
       }
       lab8 = u8.ptr;
       device_steps(lab8, host_of);
+      // on the solver's (non-blocking) stream, after the kernels that set it
       int flag = 0;
-      check_cuda(cudaMemcpy(&flag, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost), "labels check");
+      check_cuda(cudaMemcpyAsync(&flag, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                 "labels check");
+      check_cuda(cudaStreamSynchronize(stream_), "labels check");
       if (flag) throw invalid_argument("labels must index into `indices`");
     } else {
       device_steps(lab8, host_of);
@@ -462,9 +466,12 @@ void PlaneSolver<T>::setup() {
     if (thr2d_ > kPlaneThreads || nn * sizeof(C) > 227 * 1024)
       throw invalid_argument("ny too large for the single-CTA line transform");
     thr_line3_ = thr2d_;
+    line_ept8_ = threads_needed(hy_.plan, 1, 8) <= kPlaneThreads;
+    if (line_ept8_) thr_line3_ = std::max(64, threads_needed(hy_.plan, 1, 8));
     check_cuda(cudaFuncSetAttribute(k_step2d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
-    check_cuda(cudaFuncSetAttribute(k_line_fft<-1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
-    check_cuda(cudaFuncSetAttribute(k_line_fft<1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+    for (auto k : {(const void*)k_line_fft<-1, T>, (const void*)k_line_fft<1, T>,
+                   (const void*)k_line_fft<-1, T, 8>, (const void*)k_line_fft<1, T, 8>})
+      check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
   } else {
     rows2_ = rows_shape(2, 8);
     rows3_ = rows_shape(3, 8);
@@ -814,12 +821,18 @@ template <typename T>
 void PlaneSolver<T>::fft_plane(const C* in, C* out, int ncomp, int dir) {
   const int ny = static_cast<int>(in_.ny), nx = static_cast<int>(in_.nx);
   if (is2d()) {
-    if (dir < 0)
-      launch(k_line_fft<-1, T>, dim3(ncomp), dim3(thr_line3_), n() * sizeof(C), in, out, ny, ncomp,
-             hy_.plan, tw_y_.ptr);
-    else
-      launch(k_line_fft<1, T>, dim3(ncomp), dim3(thr_line3_), n() * sizeof(C), in, out, ny, ncomp,
-             hy_.plan, tw_y_.ptr);
+    const std::size_t sm = n() * sizeof(C);
+    if (line_ept8_) {
+      if (dir < 0)
+        launch(k_line_fft<-1, T, 8>, dim3(ncomp), dim3(thr_line3_), sm, in, out, ny, ncomp, hy_.plan, tw_y_.ptr);
+      else
+        launch(k_line_fft<1, T, 8>, dim3(ncomp), dim3(thr_line3_), sm, in, out, ny, ncomp, hy_.plan, tw_y_.ptr);
+    } else {
+      if (dir < 0)
+        launch(k_line_fft<-1, T>, dim3(ncomp), dim3(thr_line3_), sm, in, out, ny, ncomp, hy_.plan, tw_y_.ptr);
+      else
+        launch(k_line_fft<1, T>, dim3(ncomp), dim3(thr_line3_), sm, in, out, ny, ncomp, hy_.plan, tw_y_.ptr);
+    }
     return;
   }
   const LaunchShape& rs = ncomp == 3 ? rows3_ : rows2_;
@@ -1277,15 +1290,17 @@ void PlaneSolver<T>::run(const cd* field, int iterations, const std::int64_t* ke
     check_cuda(cudaMemcpy(&hs, gst_.ptr, sizeof(GmresState), cudaMemcpyDeviceToHost), "gmres state");
     gmres_applies_ += hs.applies;
     char* base = reinterpret_cast<char*>(gst_.ptr);
-    check_cuda(cudaMemset(base + offsetof(GmresState, err), 0, sizeof(int)), "gmres state");
-    check_cuda(cudaMemset(base + offsetof(GmresState, applies), 0, sizeof(long long)), "gmres state");
+    check_cuda(cudaMemsetAsync(base + offsetof(GmresState, err), 0, sizeof(int), stream_),
+               "gmres state");
+    check_cuda(cudaMemsetAsync(base + offsetof(GmresState, applies), 0, sizeof(long long), stream_),
+               "gmres state");
     if (hs.err) throw std::runtime_error("GMRES did not converge in the Born step (CUDA)");
   }
   if (status_.ptr) {
     int st = 0;
     check_cuda(cudaMemcpy(&st, status_.ptr, sizeof(int), cudaMemcpyDeviceToHost), "status");
     if (st) {
-      check_cuda(cudaMemset(status_.ptr, 0, sizeof(int)), "status");
+      check_cuda(cudaMemsetAsync(status_.ptr, 0, sizeof(int), stream_), "status");
       throw std::runtime_error("a bulk copy of the 3D slab step did not complete in time");
     }
   }
