@@ -469,6 +469,8 @@ void PlaneSolver<T>::setup() {
     line_ept8_ = threads_needed(hy_.plan, 1, 8) <= kPlaneThreads;
     if (line_ept8_) thr_line3_ = std::max(64, threads_needed(hy_.plan, 1, 8));
     check_cuda(cudaFuncSetAttribute(k_step2d<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+    check_cuda(cudaFuncSetAttribute(k_step2d<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
+    if (line_ept8_) thr2d_ = thr_line3_;
     for (auto k : {(const void*)k_line_fft<-1, T>, (const void*)k_line_fft<1, T>,
                    (const void*)k_line_fft<-1, T, 8>, (const void*)k_line_fft<1, T, 8>})
       check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "smem");
@@ -752,7 +754,10 @@ void PlaneSolver<T>::step(int s, bool backward, bool reflect, const C* in, C* ou
     a.n = static_cast<int>(n());
     a.store_spec = want_spec ? 1 : 0;
     a.inv_n = inv_n;
-    launch(k_step2d<T>, dim3(2), dim3(thr2d_), n() * sizeof(C), a, ps, npass, hy_.plan, tw_y_.ptr);
+    if (line_ept8_)
+      launch(k_step2d<T, 8>, dim3(2), dim3(thr2d_), n() * sizeof(C), a, ps, npass, hy_.plan, tw_y_.ptr);
+    else
+      launch(k_step2d<T>, dim3(2), dim3(thr2d_), n() * sizeof(C), a, ps, npass, hy_.plan, tw_y_.ptr);
     return;
   }
   const int ny = static_cast<int>(in_.ny), nx = static_cast<int>(in_.nx);
