@@ -158,4 +158,21 @@ inline void keep_pool_memory(int device) {
   cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
 }
 
+// Device memory free for new allocations: what the driver reports free plus what the device's
+// default pool holds reserved but unused (kept by keep_pool_memory, so a process that freed
+// buffers does not see its own cached memory as taken).
+inline std::size_t free_device_bytes(int device) {
+  std::size_t free_b = 0, total_b = 0;
+  check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used)
+      free_b += static_cast<std::size_t>(reserved - used);
+  }
+  return free_b;
+}
+
 }  // namespace bwpm

@@ -2,7 +2,11 @@
 //
 // Requests arrive at any time (submit2d/submit3d). Host preparation workers build each 2D
 // request's step records (pairs, pair-id planes, interface lists) off the launch path and price
-// its device memory exactly. A launcher admits prepared requests in arrival order while the
+// its device memory exactly. Waiting requests are taken longest estimated chain first (slab
+// steps × transform cost; ties in arrival order): the resident engine keeps each solve's SMs
+// for its whole chain, so the wall time of a burst is set by its longest chain, which should
+// start first (lengths without a compiled kernel run on the run-time-length kernels, ≈ 2.5×
+// slower per step). A launcher admits prepared requests in that order while the
 // device-memory budget holds (a request larger than the whole budget runs alone): the 2D
 // requests admitted together form a launch group, one batched launch of the resident engine on
 // its own streams (stream-ordered allocations, no device-wide synchronisation), so groups
@@ -16,6 +20,7 @@
 // The reference has no server: it solves one problem per CudaSolver.run call
 // (cpp/src/solver_cuda.cu:729-853).
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -27,6 +32,7 @@
 
 #include "devbuf.hpp"
 #include "server.hpp"
+#include "variants.hpp"
 
 namespace bwpm {
 namespace {
@@ -48,12 +54,30 @@ struct Request {
   std::vector<cd> field3;
   int iters3 = 0;
   std::size_t bytes = 0;
+  double cost = 0;  // estimated device time of the chain (relative units)
   Clock::time_point arrival, launched, finished;
   enum State { kQueued, kReady, kRunning, kDone, kFailed } state = kQueued;
   std::string error;
   ServedResult res;
 };
 using Req = std::shared_ptr<Request>;
+
+// Order of the waiting queues: longest estimated chain first, then arrival.
+bool before(const Req& a, const Req& b) {
+  return a->cost != b->cost ? a->cost > b->cost : a->id < b->id;
+}
+
+// Slab steps × transform work of a solve: steps × n·log2(n), the 2D lengths without a compiled
+// kernel of the resident engine (run-time-length kernels) at 2.5× per step.
+double chain_cost(double steps, double n, bool compiled) {
+  return steps * n * std::log2(std::max(2.0, n)) * (compiled ? 1.0 : 2.5);
+}
+
+bool has_compiled_kernel(int n) {
+  for (const auto& v : fixed_variants())
+    if (v.n == n) return true;
+  return false;
+}
 
 struct Group {
   std::unique_ptr<Batch2D> batch;
@@ -76,11 +100,8 @@ class ServerImpl final : public Server {
   explicit ServerImpl(const ServerOptions& o) : opt_(o) {
     check_cuda(cudaSetDevice(opt_.device), "cudaSetDevice");
     keep_pool_memory(opt_.device);
-    if (opt_.budget_bytes == 0) {
-      std::size_t free_b = 0, total_b = 0;
-      check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-      opt_.budget_bytes = static_cast<std::size_t>(0.8 * static_cast<double>(free_b));
-    }
+    if (opt_.budget_bytes == 0)  // free memory counts the pool's cached, unused memory
+      opt_.budget_bytes = static_cast<std::size_t>(0.8 * static_cast<double>(free_device_bytes(opt_.device)));
     opt_.max_groups = std::max(1, opt_.max_groups);
     opt_.max_group_solves = std::max(1, opt_.max_group_solves);
     opt_.max_3d = std::max(1, opt_.max_3d);
@@ -104,6 +125,7 @@ class ServerImpl final : public Server {
 
   std::int64_t submit2d(Solve2D s, const std::int32_t* labels) override {
     auto r = std::make_shared<Request>();
+    r->cost = chain_cost(2.0 * std::max(1, s.iterations) * s.nz, s.ny, has_compiled_kernel(s.ny));
     r->s2 = std::move(s);
     r->borrowed = labels;
     return enqueue(std::move(r));
@@ -116,6 +138,8 @@ class ServerImpl final : public Server {
     auto r = std::make_shared<Request>();
     r->is3d = true;
     r->borrowed = labels;
+    r->cost = chain_cost(2.0 * std::max(1, iterations) * static_cast<double>(in.nz),
+                         static_cast<double>(in.ny * in.nx), true);
     in.device = opt_.device;
     r->s3 = std::move(in);
     r->field3 = std::move(field);
@@ -184,8 +208,9 @@ class ServerImpl final : public Server {
         std::unique_lock<std::mutex> lk(mu_);
         cv_.wait(lk, [&] { return stop_ || !incoming_.empty(); });
         if (incoming_.empty()) return;
-        r = incoming_.front();
-        incoming_.pop_front();
+        auto it = std::min_element(incoming_.begin(), incoming_.end(), before);
+        r = *it;
+        incoming_.erase(it);
       }
       std::string err;
       try {
@@ -210,16 +235,14 @@ class ServerImpl final : public Server {
         fail(r, err);
       } else {
         r->state = Request::kReady;
-        // keep the admission queue in arrival order (workers finish out of order)
-        auto pos = std::upper_bound(ready_.begin(), ready_.end(), r,
-                                    [](const Req& a, const Req& b) { return a->id < b->id; });
-        ready_.insert(pos, r);
+        // keep the admission queue in its order (workers finish out of order)
+        ready_.insert(std::upper_bound(ready_.begin(), ready_.end(), r, before), r);
       }
       cv_.notify_all();
     }
   }
 
-  // Admits ready requests in arrival order while memory allows; 2D requests form one group.
+  // Admits ready requests in queue order while memory allows; 2D requests form one group.
   // Caller holds mu_.
   void admit(std::vector<Req>& group, std::vector<Req>& runs3d) {
     std::size_t taken = 0;

@@ -2,7 +2,8 @@
 
 A `Server` takes requests at any time (`submit`) and returns a ticket at once. 2D requests (the
 reference's 2D convention, src/bwpm/fast.py:120-142) are prepared on host worker threads,
-admitted in arrival order while the device-memory budget holds, and launched in groups on the
+admitted longest estimated chain first (then in arrival order) while the device-memory budget
+holds, and launched in groups on the
 batched resident engine (complex64 fields, FP64 tables and power flux); groups launched while
 others are still running share the GPU. 3D requests run through the complex64 plane engine on
 their own streams. Every result carries its latency (submit → result on the host), its queueing

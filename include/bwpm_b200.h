@@ -140,8 +140,9 @@ void bwpm_batch_destroy(bwpm_batch* b);
 /* ---- served request loop (continuous batching; no counterpart in the reference, which solves
  * one problem per CudaSolver.run call: cpp/src/solver_cuda.cu:729-853) ----------------------
  * Requests are submitted at any time and return a ticket at once. 2D requests (the reference's
- * 2D convention, src/bwpm/fast.py:120-142) are prepared on host worker threads, admitted in
- * arrival order while the device-memory budget holds, and launched in groups on the batched
+ * 2D convention, src/bwpm/fast.py:120-142) are prepared on host worker threads, admitted
+ * longest estimated chain first (then in arrival order) while the device-memory budget holds,
+ * and launched in groups on the batched
  * resident engine; groups launched while others run share the GPU. 3D requests run through the
  * complex64 plane engine on their own streams. budget_bytes 0: 80 % of the free device memory;
  * max_groups / max_group_solves / max_3d ≤ 0: defaults (8, 64, 16). Destroying the server waits
