@@ -7,6 +7,7 @@
 // and E_y (m11). Work items (solve, component) are grouped into size classes by CTA width; each
 // class is one persistent kernel on its own stream, all launched together.
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -32,7 +33,7 @@ namespace {
 constexpr int kClassThreads[] = {64, 128, 256, 512};
 constexpr int kGenericClasses = 4;
 constexpr int kMaxFixedLengths = 28;
-constexpr int kMaxRt = 10;
+constexpr int kMaxRt = 12;
 constexpr int kRtBase = kGenericClasses + kMaxFixedLengths;  // classes of the run-time-length kernels
 constexpr int kNumClasses = kRtBase + kMaxRt;  // [4, kRtBase): fixed lengths, then E values
 constexpr int kTuneScale = 4;     // autotuning runs keep 1/kTuneScale of every chain
@@ -85,21 +86,29 @@ std::vector<int> rt_radices(int n, int e) {
 
 // Position in rt_variants() of the run-time-length kernel for length n, or −1: among the E
 // that divide n within the kernel's thread limit, the smallest estimated per-thread work over
-// the stages (measured: more threads with fewer values each beat fewer stages).
+// the stages (measured: more threads with fewer values each beat fewer stages). A wide form
+// counts only where its default form cannot run n, and at 1.2× its estimate (its 128 registers
+// spill: 3645 points run faster with E = 15 on 243 threads than with wide E = 9 on 405).
+// BWPM_RT_E=<E> (tuning measurements) takes the kernel with that E where it can run n.
 int rt_choice(int n) {
   const auto& rv = rt_variants();
   if (rt_smem_bytes(n) > 220 * 1024) return -1;
   int best = -1;
   double best_score = 1e30;
+  const char* force = std::getenv("BWPM_RT_E");
+  const int forced_e = force ? std::atoi(force) : 0;
   for (std::size_t i = 0; i < rv.size(); ++i) {
     const int e = rv[i].e;
-    if (n % e || n / e > rg::rt_max_threads(e)) continue;
+    const bool wide = rv[i].max_threads > rg::rt_max_threads(e);
+    if (n % e || n / e > rv[i].max_threads || (wide && n / e <= rg::rt_max_threads(e))) continue;
     const std::vector<int> r = rt_radices(n, e);
     if (r.empty()) continue;
+    if (e == forced_e) return static_cast<int>(i);
     // a stage costs about (8 + E) value-times per thread (E values plus fixed overhead), twice
     // for a gather stage
     double score = 0;
     for (int x : r) score += (e % x == 0 ? 1.0 : 2.0) * (8.0 + e);
+    if (wide) score *= 1.2;
     if (score < best_score - 1e-9) {
       best_score = score;
       best = static_cast<int>(i);

@@ -306,9 +306,12 @@ __host__ __device__ constexpr std::size_t rt_smem_bytes(int n) {
          2 * static_cast<std::size_t>(n) * sizeof(float);  // + the mask
 }
 
-// Persistent kernel over items of any length n = E·nt (nt ≤ blockDim, plan per item).
-template <int E>
-__global__ void __launch_bounds__(rg::rt_max_threads(E), 1)
+// Persistent kernel over items of any length n = E·nt (nt ≤ blockDim, plan per item). NTMAX:
+// the thread limit (and so the register budget) of the instance; 512 for a small E is the wide
+// form for lines whose n/E exceeds the default limit (128 registers: it spills, but a line of
+// 4050 points then runs on 450 threads with E = 9 instead of 135 with E = 30: 57 → 36 µs a step).
+template <int E, int NTMAX = rg::rt_max_threads(E)>
+__global__ void __launch_bounds__(NTMAX, 1)
     k_resident2d_rt(const R2Item* __restrict__ items, int nitems, int* queue, R2Shared sh) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_item;

@@ -27,6 +27,7 @@ const std::vector<FixedVariant>& fixed_variants();
 struct RtVariant {
   int e;
   const void* fn;
+  int max_threads;  // the instance's thread limit (rg::rt_max_threads(e), or 512: wide form)
 };
 const std::vector<RtVariant>& rt_variants();
 
