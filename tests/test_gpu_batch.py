@@ -285,7 +285,7 @@ def test_autotuned_batch_equals_forced_variant():
         assert np.array_equal(b.result(i)["transmitted"], forced.result(j)["transmitted"])
 
 
-@pytest.mark.parametrize("n", [1000, 1125, 1200, 1944, 2160, 2187, 3645, 4000, 3125])
+@pytest.mark.parametrize("n", [1000, 1125, 1200, 1944, 2160, 2187, 2700, 3645, 4000, 4050, 3125])
 def test_runtime_length_kernels_match_fp64(n):
     """Lengths without a compiled kernel: the run-time-length register kernels (E values per
     thread, radices 2/3/4/5/8 dividing E), or the generic kernel (3125 = 5^5), against FP64."""
@@ -302,6 +302,19 @@ def test_runtime_length_kernels_match_fp64(n):
     r = b.result(i)
     assert rel_l2(r["transmitted"], ref["transmitted"][:, 0]) < L2_C64, cls
     assert rel_l2(r["reflected"], ref["reflected"][:, 0]) < L2_C64, cls
+
+
+def test_wide_runtime_length_kernel_runs_4050_points():
+    """4050 = 2·3⁴·5²: the default kernels with E ≥ 9 take at most 256 threads, where only E = 30
+    (135 threads) fits; the wide form (512 threads) runs it with E = 9 on 450 threads."""
+    from bwpm_b200.batch import Batch2D
+
+    p = _variant_problem(4050)
+    b = Batch2D()
+    b.add_problem(p)
+    b.prepare()
+    cls = b.classes()[0]
+    assert cls["variant"] <= -2 and 256 < cls["threads"] <= 512, cls
 
 
 @pytest.mark.parametrize("n", [1024, 2048])
