@@ -271,3 +271,26 @@ def test_born_step_graph_born2d(core, monkeypatch, precision):
                                     precision=precision).run(p.field, p.iterations, [])
     for key in ("transmitted", "reflected"):
         assert np.array_equal(out["host"][key], out["graph"][key]), key
+
+
+@pytest.mark.parametrize("mode", ["graph", "host"])
+def test_born_gmres_restart_limit_raises(core, monkeypatch, mode):
+    """A GMRES(30) that cannot converge (tolerance 0) stops after 100 restarts with RuntimeError,
+    as the reference does (cpp/src/solver.cpp:341-342). In the Born-step graph the limit sets an
+    error flag that the run reads at its end; the next solver on the device runs normally."""
+    monkeypatch.setenv("BWPM_GMRES", mode)
+    # ≈ 400 propagating modes per component: no Krylov breakdown (an exact solve) within a cycle
+    ny, lam = 1024, 0.633e-3
+    dy = lam / 8
+    dz = lam / 10
+    y = (np.arange(ny) - ny // 2) * dy
+    field = np.zeros((ny, 1, 2), complex)
+    field[:, 0, 0] = np.exp(-((y / (64 * dy)) ** 2))
+    labels = np.zeros((1, ny, 1), np.int32)
+    fl = 0.01 * np.random.default_rng(3).standard_normal((1, ny, 1)) + 0j
+    args = (ny, 1, dy, 1.0, dz, 2 * np.pi / lam, np.array([1.5 + 0j]), labels, 1.0 + 0j, None)
+    s = core.CudaSolver(*args, 0, fluctuation=fl, gmres_tol=0.0)
+    with pytest.raises(RuntimeError, match="GMRES did not converge"):
+        s.run(field, 0, [])
+    r = core.CudaSolver(*args, 0, fluctuation=fl).run(field, 0, [])
+    assert np.all(np.isfinite(r["transmitted"])) and np.linalg.norm(r["transmitted"]) > 0
