@@ -82,3 +82,31 @@ def test_fixed_length_kernels_are_deterministic(monkeypatch):
     b = _run(monkeypatch, 512, 512, 30, "facet", 32, "fixed")
     for key in ("transmitted", "reflected"):
         assert np.array_equal(a[key], b[key]), key
+
+
+def test_fixed_length_kernels_born_3d(monkeypatch):
+    """A 3D Born chain (δn on every slab of a 256² plane): the fixed-length column kernel also
+    writes the step's spectrum that the Born step starts from. Complex64 through the fixed-length
+    kernels against the general ones and against FP64."""
+    from bwpm_b200 import _core, workloads
+
+    n, nz, lam = 256, 6, 0.633e-3
+    d, dz = lam / 6, lam / 8
+    c = workloads.centred(n, d)
+    field = np.zeros((n, n, 2), complex)
+    field[..., 0] = np.exp(-(c[:, None] ** 2 + c[None, :] ** 2) / (n * d / 8) ** 2)
+    labels = np.zeros((nz, n, n), np.int32)
+    rng = np.random.default_rng(11)
+    fl = 0.01 * rng.standard_normal((nz, n, n)) + 0j
+    args = (n, n, d, d, dz, workloads.k0_of(0.633), np.array([1.5 + 0j]), labels, 1.0 + 0j, None)
+    out = {}
+    for name, prec, kernels in (("rf", 32, None), ("gen", 32, "general"), ("f64", 64, "general")):
+        if kernels:
+            monkeypatch.setenv("BWPM_3D_KERNELS", kernels)
+        else:
+            monkeypatch.delenv("BWPM_3D_KERNELS", raising=False)
+        out[name] = _core.CudaSolver(*args, 0, fluctuation=fl, precision=prec).run(field, 1, [])
+    for key in ("transmitted", "reflected"):
+        assert np.linalg.norm(out["f64"][key]) > 0, key
+        assert rel_l2(out["rf"][key], out["f64"][key]) < C64_TOL, (key, rel_l2(out["rf"][key], out["f64"][key]))
+        assert rel_l2(out["rf"][key], out["gen"][key]) < FORMS_TOL, (key, rel_l2(out["rf"][key], out["gen"][key]))
