@@ -10,7 +10,7 @@ these fixtures:
 2. Extra cases computed by the reference itself:
    - the random volumes of the reference's CUDA parity tests (tests/test_core_cuda.py:91-196),
      run through the reference's Python `Bidirectional3D` (src/bwpm/volume3d.py:246-319);
-   - BASELINE-shaped cases (the 2D slab at full size, reduced Born and 3D microlens cases), run
+   - workload-shaped cases (the 2D slab at full size, reduced Born and 3D microlens cases), run
      through the reference's compiled CPU core `bwpm._core.Solver` (cpp/src/solver.cpp:444-528)
      built by oracle/build_ref.sh.
 
