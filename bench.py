@@ -479,10 +479,10 @@ def _summary(line: dict) -> dict:
         "served_solves_per_s": get(line, "served", "solves_per_s"),
         "served_p50_p99_ms": [get(line, "served", "p50_ms"), get(line, "served", "p99_ms")],
         "served_speedup_vs_fp64": get(line, "served", "speedup_vs_fp64_plain"),
-        "cfg1_ms_c64_both_fp64_each": [get(cfg, "slab2d", "c64_batched_ms_both"),
+        "slab2d_ms_c64_both_fp64_each": [get(cfg, "slab2d", "c64_batched_ms_both"),
                                        get(cfg, "slab2d", "fp64_ms_per_solve")],
-        "cfg2_s_c64_fp64": [get(cfg, "born2d", "c64_s"), get(cfg, "born2d", "fp64_s")],
-        "cfg3_s_c64_fp64_refcuda": [get(cfg, "microlens3d", "c64_s"), get(cfg, "microlens3d", "fp64_s"),
+        "born2d_s_c64_fp64": [get(cfg, "born2d", "c64_s"), get(cfg, "born2d", "fp64_s")],
+        "microlens3d_s_c64_fp64_refcuda": [get(cfg, "microlens3d", "c64_s"), get(cfg, "microlens3d", "fp64_s"),
                                     get(cfg, "microlens3d", "reference_cuda_fp64_s")],
     }
 
@@ -620,10 +620,10 @@ def _reference_cuda_core():
 
 
 def run_configs(device: int) -> dict:
-    """Configurations 1-3 on this GPU: the complex64 result of this implementation against the
-    per-solve FP64 drop-in path (time and relative L2 error), the reference's own GPU core
-    (cuFFT, FP64; staged build) on the same solves, and for the 2D slab the reference's CPU core
-    on one thread. Configuration 2 (Born) runs at full size in TE; times include set-up."""
+    """The slab, Born and microlens workloads on this GPU: the complex64 result of this
+    implementation against the per-solve FP64 drop-in path (time and relative L2 error), the
+    reference's own GPU core (cuFFT, FP64; staged build) on the same solves, and for the 2D slab
+    the reference's CPU core on one thread. The Born chain runs at full size in TE; times include set-up."""
     from bwpm_b200 import _core, workloads
     from bwpm_b200.batch import Batch2D
 
@@ -748,7 +748,7 @@ def main() -> None:
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="instances per step of the CPU reference (default: 3 per host core)")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream measurement")
-    ap.add_argument("--no-configs", action="store_true", help="skip configurations 1-3")
+    ap.add_argument("--no-configs", action="store_true", help="skip the slab, Born and microlens workloads")
     ap.add_argument("--served-fp64", type=int, default=16, help="FP64 sample of the served stream")
     ap.add_argument("--variants", type=str, default="",
                     help="profiling only: NY:VARIANT,... forces kernel variants (no autotuning)")

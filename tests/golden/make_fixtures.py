@@ -15,7 +15,7 @@ these fixtures:
      built by oracle/build_ref.sh.
 
 Usage: python tests/golden/make_fixtures.py          (golden files, random volumes, workloads)
-       python tests/golden/make_fixtures.py full     (configurations 2 and 3 at full size)
+       python tests/golden/make_fixtures.py full     (the Born chain and the microlens at full size)
        python tests/golden/make_fixtures.py post     (post-processing of fields)
 """
 
@@ -268,7 +268,7 @@ def _full_case(name: str):
 
 
 def full_size_cases() -> None:
-    """Configurations 2 and 3 at full size through the reference CPU core, FP64:
+    """The Born chain and the 3D microlens at full size through the reference CPU core, FP64:
     - born2d_te / born2d_tm: 4096 points, 2000 slabs with δn on every slab, 6 iterations
       (inputs from bwpm_b200.workloads.born2d, seed 2): full transmitted and reflected fields
       and the norms of the per-iteration fields;

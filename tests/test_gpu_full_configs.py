@@ -1,4 +1,4 @@
-"""Configurations 2 and 3 at full size against the reference CPU core (on a GPU).
+"""The 2D Born chain and the 3D microlens at full size against the reference CPU core (on a GPU).
 
 Fixture tests/golden/full_configs.npz (tests/golden/make_fixtures.py `full`): the reference's
 compiled CPU core (cpp/src/solver.cpp:444-528) on
@@ -10,7 +10,7 @@ compiled CPU core (cpp/src/solver.cpp:444-528) on
 FP64 at relative L2 ≤ 1e-10; complex64 at ≤ 1e-4 (the Born reflected field: 1e-3, see
 C64_TOL_BORN_REFLECTED). Behind the silver the transmitted field is
 ≈ 1e-94 of the incident one, below the complex64 range (its smallest normal is ≈ 1e-38), so the
-complex64 transmitted field of configuration 3 is checked against a floor of 1e-6 of the
+complex64 transmitted field of the microlens is checked against a floor of 1e-6 of the
 incident field's norm: ‖E − E_ref‖ ≤ 1e-4 · max(‖E_ref‖, 1e-6 ‖E_in‖).
 """
 

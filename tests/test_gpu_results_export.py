@@ -1,6 +1,6 @@
 """A GPU result exported in the reference's golden-file envelope and read back (on a GPU).
 
-Configuration 1 at full size (1024 points, 250 slabs, 8 iterations, TE and TM) runs through the
+The 5 µm slab at full size (1024 points, 250 slabs, 8 iterations, TE and TM) runs through the
 FP64 drop-in path and the batched complex64 engine; each result becomes a `FieldReference`
 record (bwpm_b200.results.solve_record) in a "raytatouille-result" file, which is read back by
 this package and, where the reference package is staged (oracle/stage_reference.sh), by the
